@@ -1,0 +1,236 @@
+"""ctypes binding of the native engine ``libgpusw_sm100.so`` (C ABI in include/gpusw_b200.h).
+
+This is the only module that talks to the GPU. It replaces the reference package's CuPy
+boundary (``src/gpusw/_compile.py`` and ``src/gpusw/backends/cuda.py``): there is no
+runtime compilation and no CPU fallback -- if the shared library is missing or no device
+is visible, the scoring calls raise :class:`~gpusw_b200.errors.NoGpuError`.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+from .errors import GpuSWError, NoGpuError, OverflowRiskError, SchemeError
+
+__all__ = ["LIB_PATH", "load", "gpu_available", "Context", "context", "Stats"]
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libgpusw_sm100.so")
+
+OK, E_INVALID, E_NO_GPU, E_CUDA, E_MEMORY, E_OVERFLOW, E_SCHEME = 0, 1, 2, 3, 4, 5, 6
+E_QUEUE_FULL, E_NOT_FOUND, E_CANCELLED, E_TIMEOUT = 7, 8, 9, 10
+DTYPE_CODES = {"auto": 0, "int16": 1, "int32": 2}
+MODE_CODES = {"local": 0, "global": 1, "semiglobal": 2}
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("last_kernel_ms", ctypes.c_double),
+        ("last_total_ms", ctypes.c_double),
+        ("last_cells", ctypes.c_double),
+        ("last_pairs", ctypes.c_int64),
+        ("last_overflow", ctypes.c_int64),
+        ("last_launches", ctypes.c_int64),
+        ("total_launches", ctypes.c_int64),
+        ("total_overflow", ctypes.c_int64),
+        ("device_bytes", ctypes.c_int64),
+    ]
+
+
+_SIGNATURES = {
+    "gpusw_version": ([], ctypes.c_int),
+    "gpusw_device_count": ([ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "gpusw_ctx_create": ([ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "gpusw_ctx_destroy": ([ctypes.c_void_p], None),
+    "gpusw_last_error": ([ctypes.c_void_p], ctypes.c_char_p),
+    "gpusw_set_scheme": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                          ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "gpusw_db_upload": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                         ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
+    "gpusw_db_free": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
+    "gpusw_db_bits": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
+    "gpusw_score_cross": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+                           ctypes.c_int32, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "gpusw_topk": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+                    ctypes.c_int32, ctypes.c_int32, ctypes.c_int, ctypes.c_void_p,
+                    ctypes.c_void_p], ctypes.c_int),
+    "gpusw_score_pairs": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+                           ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p],
+                          ctypes.c_int),
+    "gpusw_set_options": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int64], ctypes.c_int),
+    "gpusw_get_stats": ([ctypes.c_void_p, ctypes.POINTER(Stats)], ctypes.c_int),
+    "gpusw_sync": ([ctypes.c_void_p], ctypes.c_int),
+    "gpusw_measure_dpx_rate": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+    "gpusw_flush_l2": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+}
+
+
+def load():
+    """Load the shared library (once); raise NoGpuError if it is not built."""
+    global _lib
+    with _lib_lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise NoGpuError(
+                    f"native engine {LIB_PATH} is not built; run `python -c \"import "
+                    "__graft_entry__ as g; g.build()\"` or `python -m gpusw_b200.build`")
+            lib = ctypes.CDLL(LIB_PATH)
+            for name, (args, res) in _SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.argtypes = args
+                fn.restype = res
+            _lib = lib
+    return _lib
+
+
+def gpu_available() -> bool:
+    """True iff the native engine loads and at least one CUDA device is visible."""
+    try:
+        lib = load()
+    except (NoGpuError, OSError):
+        return False
+    n = ctypes.c_int(0)
+    return lib.gpusw_device_count(ctypes.byref(n)) == OK and n.value > 0
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _raise(code: int, msg: str):
+    if code == E_INVALID or code == E_NOT_FOUND:
+        raise ValueError(msg)
+    if code == E_NO_GPU:
+        raise NoGpuError(msg)
+    if code == E_OVERFLOW:
+        raise OverflowRiskError(msg)
+    if code == E_SCHEME:
+        raise SchemeError(msg)
+    raise GpuSWError(msg)
+
+
+class Context:
+    """One native context: a CUDA stream on one device plus the resident sequence sets."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        self.device = int(device)
+        handle = ctypes.c_void_p()
+        rc = self.lib.gpusw_ctx_create(self.device, ctypes.byref(handle))
+        if rc != OK:
+            _raise(rc, self.lib.gpusw_last_error(None).decode() or "context creation failed")
+        self.handle = handle
+        self._scheme_key = None
+        self.lock = threading.RLock()
+
+    def _check(self, rc: int):
+        if rc != OK:
+            _raise(rc, self.lib.gpusw_last_error(self.handle).decode())
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.gpusw_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------ configuration
+    def set_scheme(self, scheme) -> None:
+        key = (scheme.mode, scheme.gap_open, scheme.gap_extend, bool(scheme.free_end_gaps_query),
+               bool(scheme.free_end_gaps_ref), scheme.table_hash())
+        if key == self._scheme_key:
+            return
+        sub = np.ascontiguousarray(scheme.substitution_table(), dtype=np.int32)
+        self._check(self.lib.gpusw_set_scheme(
+            self.handle, MODE_CODES[scheme.mode], scheme.gap_open, scheme.gap_extend,
+            int(bool(scheme.free_end_gaps_query)), int(bool(scheme.free_end_gaps_ref)),
+            int(sub.shape[0]), _ptr(sub)))
+        self._scheme_key = key
+
+    def set_options(self, plain: bool = False, mem_budget: int = 0) -> None:
+        self._check(self.lib.gpusw_set_options(self.handle, int(bool(plain)), int(mem_budget)))
+
+    # ------------------------------------------------------------------ sequence sets
+    def upload(self, codes: np.ndarray, offsets: np.ndarray) -> int:
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+        n = offsets.shape[0] - 1
+        h = ctypes.c_int32(0)
+        self._check(self.lib.gpusw_db_upload(self.handle, _ptr(codes), _ptr(offsets), n,
+                                             ctypes.byref(h)))
+        return h.value
+
+    def free(self, db: int) -> None:
+        if self.handle:
+            self.lib.gpusw_db_free(self.handle, int(db))
+
+    def bits(self, db: int) -> int:
+        v = self.lib.gpusw_db_bits(self.handle, int(db))
+        if v < 0:
+            self._check(-v)
+        return v
+
+    # ----------------------------------------------------------------------- scoring
+    def score_cross(self, qdb: int, rdb: int, qlist: np.ndarray, n_refs: int, dtype: str) -> np.ndarray:
+        qlist = np.ascontiguousarray(qlist, dtype=np.int32)
+        out = np.empty((qlist.shape[0], n_refs), dtype=np.int32)
+        self._check(self.lib.gpusw_score_cross(self.handle, qdb, rdb, _ptr(qlist), qlist.shape[0],
+                                               DTYPE_CODES[dtype], _ptr(out)))
+        return out
+
+    def topk(self, qdb: int, rdb: int, qlist: np.ndarray, n_refs: int, k: int, dtype: str):
+        qlist = np.ascontiguousarray(qlist, dtype=np.int32)
+        kk = max(0, min(int(k), n_refs))
+        idx = np.empty((qlist.shape[0], kk), dtype=np.int32)
+        sc = np.empty((qlist.shape[0], kk), dtype=np.int32)
+        self._check(self.lib.gpusw_topk(self.handle, qdb, rdb, _ptr(qlist), qlist.shape[0], int(k),
+                                        DTYPE_CODES[dtype], _ptr(idx), _ptr(sc)))
+        return idx, sc
+
+    def score_pairs(self, qdb: int, rdb: int, qi: np.ndarray, rj: np.ndarray, dtype: str) -> np.ndarray:
+        qi = np.ascontiguousarray(qi, dtype=np.int32)
+        rj = np.ascontiguousarray(rj, dtype=np.int32)
+        out = np.empty(qi.shape[0], dtype=np.int32)
+        self._check(self.lib.gpusw_score_pairs(self.handle, qdb, rdb, _ptr(qi), _ptr(rj),
+                                               qi.shape[0], DTYPE_CODES[dtype], _ptr(out)))
+        return out
+
+    # ------------------------------------------------------------------- measurement
+    def stats(self) -> Stats:
+        s = Stats()
+        self._check(self.lib.gpusw_get_stats(self.handle, ctypes.byref(s)))
+        return s
+
+    def sync(self) -> None:
+        self._check(self.lib.gpusw_sync(self.handle))
+
+    def dpx_rate(self) -> float:
+        v = ctypes.c_double(0.0)
+        self._check(self.lib.gpusw_measure_dpx_rate(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def flush_l2(self, nbytes: int = 256 << 20) -> None:
+        self._check(self.lib.gpusw_flush_l2(self.handle, int(nbytes)))
+
+
+_contexts: dict[int, Context] = {}
+_ctx_lock = threading.Lock()
+
+
+def context(device: int = 0) -> Context:
+    """The process-wide context of ``device`` (created on first use)."""
+    with _ctx_lock:
+        ctx = _contexts.get(int(device))
+        if ctx is None:
+            ctx = Context(device)
+            _contexts[int(device)] = ctx
+        return ctx

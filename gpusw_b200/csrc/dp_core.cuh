@@ -1,0 +1,346 @@
+// Gotoh affine-gap scoring on sm_100a: the team wavefront core.
+//
+// Recurrence (same integers as the reference package's kernel, src/gpusw/kernel.py:56-158,
+// and oracle, src/gpusw/reference.py:38-125): rows i run over the row sequence (the
+// reference in a cross product), columns j over the column sequence (the query),
+//   F(i,j) = max(H(i-1,j) + go, F(i-1,j) + ge)
+//   E(i,j) = max(H(i,j-1) + go, E(i,j-1) + ge)
+//   H(i,j) = max(H(i-1,j-1) + SUB[r_i][q_j], E, F)   (and >= 0 in local mode)
+//
+// Layout. A "team" of G lanes (G = 8, 16 or 32 consecutive lanes of one warp) scores one
+// alignment task; lane L owns the W consecutive columns [L*W, L*W + W) of the current
+// column pass and keeps their vertical state in registers. Row i reaches lane L at step
+// t = i + L (anti-diagonal wavefront); the horizontal carry of each row travels one lane
+// to the right per step through __shfl_up_sync, and so does the row's residue code.
+//
+// Packing. With P = 2 every 32-bit register holds two int16 cells of two different
+// alignments (the column sequences c0, c1 of a pair against the same row sequence in a
+// cross product, or two unrelated pairs), updated together by the DPX s16x2 instructions.
+// With P = 1 a register holds one int32 cell (the int32 path and the overflow rerun).
+//
+// Algebra used to shorten the per-column dependency chain (exact over the integers):
+//   HGO = H + go is stored instead of H, and the profile holds s' = s - go, so that
+//   X(i,j)   = max(HGO(i-1,j-1) + s', F(i,j) [, 0 in local mode])    (= max(Hdiag+s, F))
+//   E(i,j)   = max(E(i,j-1) + max(ge, go), X(i,j-1) + go)             (H = max(X, E))
+//   HGO(i,j) = max(E(i,j) + go, X(i,j) + go)
+// so the only serial dependency along a row is one add-max per column (the E chain).
+// Cost per cell register: F, X, X+go, E, HGO = 5 int16x2 ops, plus 1/2 op for the
+// running maximum (3-input max over two columns).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gsw {
+
+constexpr int kModeLocal = 0, kModeGlobal = 1, kModeSemi = 2;
+
+// Per-call scheme constants shared by every kernel.
+struct SchemeDev {
+  int mode;       // kModeLocal / kModeGlobal / kModeSemi
+  int free_q;     // semiglobal: free end gaps in the query (column sequence)
+  int free_r;     // semiglobal: free end gaps in the reference (row sequence)
+  int go, ge;     // gap open / extend (<= 0)
+  int ges;        // max(ge, go): E extension cost once H = max(X, E) is folded in
+  int ns;         // side of the substitution table (alphabet + sentinel)
+  int pad_code;   // profile row used for padded rows (= ns)
+  int s_pad;      // substitution score of padded cells (<= 0)
+  int ovf_limit;  // int16 runs: a score above this may have wrapped -> rescore in int32
+  int neg_e0, neg_f, neg_low;  // per-width sentinels (see make_scheme on the host)
+};
+
+// -------------------------------------------------------------------------------------
+// Lane arithmetic: P = 2 -> two int16 cells per register (DPX s16x2), P = 1 -> int32.
+template <int P> struct V;
+template <> struct V<2> {
+  static __device__ __forceinline__ uint32_t addmax(uint32_t a, uint32_t b, uint32_t c) {
+    return __viaddmax_s16x2(a, b, c);
+  }
+  static __device__ __forceinline__ uint32_t addmax_relu(uint32_t a, uint32_t b, uint32_t c) {
+    return __viaddmax_s16x2_relu(a, b, c);
+  }
+  static __device__ __forceinline__ uint32_t max3(uint32_t a, uint32_t b, uint32_t c) {
+    return __vimax3_s16x2(a, b, c);
+  }
+  static __device__ __forceinline__ uint32_t max2(uint32_t a, uint32_t b) { return __vmaxs2(a, b); }
+  static __device__ __forceinline__ uint32_t add(uint32_t a, uint32_t b) { return __vadd2(a, b); }
+  static __device__ __forceinline__ uint32_t splat(int v) { return (uint32_t)(v & 0xFFFF) * 0x10001u; }
+  static __device__ __forceinline__ uint32_t pack(int lo, int hi) {
+    return (uint32_t)(lo & 0xFFFF) | ((uint32_t)(hi & 0xFFFF) << 16);
+  }
+  static __device__ __forceinline__ int get(uint32_t w, int h) { return (int)(int16_t)(w >> (16 * h)); }
+  static __device__ __forceinline__ uint32_t half_mask(int h) { return h ? 0xFFFF0000u : 0x0000FFFFu; }
+};
+template <> struct V<1> {
+  static __device__ __forceinline__ uint32_t addmax(uint32_t a, uint32_t b, uint32_t c) {
+    return (uint32_t)__viaddmax_s32((int)a, (int)b, (int)c);
+  }
+  static __device__ __forceinline__ uint32_t addmax_relu(uint32_t a, uint32_t b, uint32_t c) {
+    return (uint32_t)__viaddmax_s32_relu((int)a, (int)b, (int)c);
+  }
+  static __device__ __forceinline__ uint32_t max3(uint32_t a, uint32_t b, uint32_t c) {
+    return (uint32_t)__vimax3_s32((int)a, (int)b, (int)c);
+  }
+  static __device__ __forceinline__ uint32_t max2(uint32_t a, uint32_t b) { return (uint32_t)max((int)a, (int)b); }
+  static __device__ __forceinline__ uint32_t add(uint32_t a, uint32_t b) { return a + b; }
+  static __device__ __forceinline__ uint32_t splat(int v) { return (uint32_t)v; }
+  static __device__ __forceinline__ uint32_t pack(int lo, int) { return (uint32_t)lo; }
+  static __device__ __forceinline__ int get(uint32_t w, int) { return (int)w; }
+  static __device__ __forceinline__ uint32_t half_mask(int) { return 0xFFFFFFFFu; }
+};
+
+// H(0, j) / H(i, 0) boundary value of a DP edge of length k (k >= 0).
+__device__ __forceinline__ int edge_value(const SchemeDev& S, bool free_edge, int k) {
+  if (k == 0 || S.mode == kModeLocal || (S.mode == kModeSemi && free_edge)) return 0;
+  return S.go + (k - 1) * S.ge;
+}
+
+// Score of a pair with an empty side (src/gpusw/reference.py:48-54).
+__device__ __forceinline__ int empty_score(const SchemeDev& S, int n, int m) {
+  if (S.mode == kModeLocal || (n == 0 && m == 0)) return 0;
+  if (n == 0) return (S.mode == kModeSemi && S.free_q) ? 0 : S.go + (m - 1) * S.ge;
+  return (S.mode == kModeSemi && S.free_r) ? 0 : S.go + (n - 1) * S.ge;
+}
+
+// Packed residue codes: sequence words start 16-byte aligned; code c of a sequence sits
+// in word c / per at bit (c % per) * bits.
+struct Packed {
+  const uint32_t* words;
+  const long long* woff;  // first word of each sequence
+  const int* len;
+  int bits, per;
+  __device__ __forceinline__ int code(int seq, int c) const {
+    uint32_t w = __ldg(words + woff[seq] + c / per);
+    return (int)((w >> ((c % per) * bits)) & ((1u << bits) - 1u));
+  }
+};
+
+// Lane 0's code feed for one row sequence: one packed word per `per` steps.
+struct RowFeed {
+  const uint32_t* ptr;
+  uint32_t cur;
+  int pos, bits, per, m, pad;
+  uint32_t mask;
+  __device__ __forceinline__ void init(const uint32_t* p, int bits_, int per_, int m_, int pad_) {
+    ptr = p; bits = bits_; per = per_; m = m_; pad = pad_; pos = 0;
+    mask = (1u << bits_) - 1u;
+    cur = m_ > 0 ? __ldg(p) : 0u;
+  }
+  // Code of row t (t = 0, 1, 2, ... called once per step); pad once past the end.
+  __device__ __forceinline__ int next(int t) {
+    int c = (int)(cur & mask);
+    cur >>= bits;
+    if (++pos == per) {
+      pos = 0;
+      ++ptr;
+      cur = (t + 1 < m) ? __ldg(ptr) : 0u;
+    }
+    return t < m ? c : pad;
+  }
+};
+
+// Per-lane accumulators of one task, merged over the column passes of the task.
+struct Acc {
+  uint32_t best;    // running max of HGO (local score / int16 overflow guard)
+  uint32_t endrow;  // max over the last row of HGO at real columns   (non-local)
+  uint32_t corner;  // HGO at (m, n)                                   (non-local)
+  uint32_t endcol;  // max over rows of HGO at column n                 (non-local, free_q)
+};
+
+// One column pass of one team task.
+//
+// prof      : shared-memory profile, row a at prof + a * pstride; uint4 slot k4*G + lane
+//             holds the 4 consecutive columns L*W + 4*k4 .. +3 of this pass (lo/hi halves
+//             are the two packed alignments when P = 2).
+// prof_hi   : second profile for PAIRS (the hi half scores against its own row codes).
+// rows      : row sequence(s); rows[1] is used only for PAIRS.
+// m0, m1    : row lengths (cross product: m1 == m0).
+// n0, n1    : full column lengths of the two halves.
+// col0      : first column (0-based) of this pass.
+// bnd       : boundary column (E, X+go) at column col0-1 for each row, read by lane 0 when
+//             has_prev, written by lane G-1 when has_next (in place: row i is read at step
+//             i and written at step i + G - 1).
+template <int G, int W, int P, bool LOCAL, bool PAIRS>
+__device__ __forceinline__ void team_pass(const SchemeDev& S, const uint4* __restrict__ prof,
+                                          int pstride, const uint32_t* row_w0,
+                                          const uint32_t* row_w1, int row_bits, int row_per,
+                                          int m0, int m1, int n0, int n1, int col0,
+                                          uint2* bnd, bool has_prev, bool has_next, int lane,
+                                          unsigned wmask, Acc& acc) {
+  using Ops = V<P>;
+  static_assert(W % 4 == 0, "W must be a multiple of 4");
+  const uint32_t GO = Ops::splat(S.go), GE = Ops::splat(S.ge), GES = Ops::splat(S.ges);
+  const uint32_t NEGF = Ops::splat(S.neg_f), NEGE0 = Ops::splat(S.neg_e0);
+  const uint32_t NEGLOW = Ops::splat(S.neg_low);
+  const int mrows = PAIRS ? max(m0, m1) : m0;
+  const bool track_endcol = !LOCAL && S.mode == kModeSemi && S.free_q;
+  const bool ladder_row0 = !(S.mode == kModeLocal || (S.mode == kModeSemi && S.free_r));
+  const bool ladder_col0 = !(S.mode == kModeLocal || (S.mode == kModeSemi && S.free_q));
+
+  // Vertical state of my W columns: HGO(0, j) and F(0, j) = -inf.
+  uint32_t HGO[W], F[W], CM[W];
+  const int jbase = col0 + lane * W;  // 0-based column of my register 0
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    int h0 = ladder_row0 ? edge_value(S, false, jbase + k + 1) : 0;
+    HGO[k] = Ops::splat(h0 + S.go);
+    F[k] = NEGF;
+    CM[k] = NEGLOW;
+  }
+  // HGO of the column left of my strip at the current row (diag of the next row).
+  uint32_t hgo_left = Ops::splat((ladder_row0 ? edge_value(S, false, jbase) : 0) + S.go);
+  // Outputs of my last column for the lane to the right.
+  uint32_t e_out = NEGE0, x_out = GO;
+  int code = S.pad_code;
+  // Lane 0 column-0 boundary: X(i,0) + go = H(i,0) + go for i >= 1.
+  uint32_t xb = Ops::splat((ladder_col0 ? S.go : 0) + S.go);
+  const uint32_t xb_step = ladder_col0 ? GE : 0u;
+
+  RowFeed f0, f1;
+  f0.init(row_w0, row_bits, row_per, m0, S.pad_code);
+  if (PAIRS) f1.init(row_w1, row_bits, row_per, m1, S.pad_code);
+
+  const int nsteps = mrows + G - 1;
+  for (int t = 0; t < nsteps; ++t) {
+    // Values the left lane produced in the previous step (row t - lane).
+    uint32_t e_in = __shfl_up_sync(wmask, e_out, 1, G);
+    uint32_t x_in = __shfl_up_sync(wmask, x_out, 1, G);
+    int c_in = __shfl_up_sync(wmask, code, 1, G);
+    int feed = f0.next(t);
+    if (PAIRS) feed |= f1.next(t) << 16;
+    const int i = t - lane;  // my row (0-based)
+    if (lane == 0) {
+      code = feed;
+      if (has_prev) {
+        uint2 b = (i < mrows) ? bnd[i] : make_uint2(NEGE0, GO);
+        e_in = b.x;
+        x_in = b.y;
+      } else {
+        e_in = NEGE0;
+        x_in = xb;
+      }
+    } else {
+      code = c_in;
+    }
+    xb = Ops::add(xb, xb_step);
+    if (i < 0 || i >= mrows) continue;
+
+    const uint4* pr0 = prof + (PAIRS ? (code & 0xFFFF) : code) * pstride + lane;
+    const uint4* pr1 = prof + (PAIRS ? (code >> 16) : code) * pstride + lane;
+    // Columns in chunks of CH: F, X and X + go (independent across columns), then the
+    // E chain (one add-max per column) and the new HGO. Chunking bounds live registers.
+    constexpr int CH = W < 16 ? W : 16;
+    uint32_t diag = hgo_left;
+    uint32_t e = Ops::addmax(e_in, GES, x_in);
+    hgo_left = Ops::addmax(e_in, GO, x_in);
+    uint32_t xlast = 0;
+#pragma unroll
+    for (int c0 = 0; c0 < W; c0 += CH) {
+      // Substitution scores s' = s - go of this chunk's columns for the row's code(s).
+      uint32_t sp[CH];
+#pragma unroll
+      for (int k4 = 0; k4 < CH / 4; ++k4) {
+        const int slot = (c0 / 4 + k4) * G;
+        const uint4 a = pr0[slot];
+        if (PAIRS) {
+          const uint4 b = pr1[slot];
+          sp[4 * k4 + 0] = (a.x & 0xFFFFu) | (b.x & 0xFFFF0000u);
+          sp[4 * k4 + 1] = (a.y & 0xFFFFu) | (b.y & 0xFFFF0000u);
+          sp[4 * k4 + 2] = (a.z & 0xFFFFu) | (b.z & 0xFFFF0000u);
+          sp[4 * k4 + 3] = (a.w & 0xFFFFu) | (b.w & 0xFFFF0000u);
+        } else {
+          sp[4 * k4 + 0] = a.x;
+          sp[4 * k4 + 1] = a.y;
+          sp[4 * k4 + 2] = a.z;
+          sp[4 * k4 + 3] = a.w;
+        }
+      }
+      uint32_t XG[CH];
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        uint32_t f = Ops::addmax(F[c0 + k], GE, HGO[c0 + k]);
+        F[c0 + k] = f;
+        uint32_t x = LOCAL ? Ops::addmax_relu(diag, sp[k], f) : Ops::addmax(diag, sp[k], f);
+        diag = HGO[c0 + k];
+        XG[k] = Ops::add(x, GO);
+      }
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        HGO[c0 + k] = Ops::addmax(e, GO, XG[k]);
+        if (c0 + k + 1 < W) e = Ops::addmax(e, GES, XG[k]);
+      }
+      xlast = XG[CH - 1];
+    }
+    e_out = e;
+    x_out = xlast;
+#pragma unroll
+    for (int k = 0; k + 1 < W; k += 2) acc.best = Ops::max3(acc.best, HGO[k], HGO[k + 1]);
+    if (has_next && lane == G - 1) bnd[i] = make_uint2(e_out, x_out);
+
+    if (!LOCAL) {
+      if (track_endcol) {
+        if (PAIRS && m0 != m1) {
+          // Rows past a half's end must not count towards that half's last column.
+          uint32_t keep = (i < m0 ? Ops::half_mask(0) : 0u) | (i < m1 ? Ops::half_mask(1) : 0u);
+#pragma unroll
+          for (int k = 0; k < W; ++k) CM[k] = Ops::max2(CM[k], (HGO[k] & keep) | (NEGLOW & ~keep));
+        } else {
+#pragma unroll
+          for (int k = 0; k < W; ++k) CM[k] = Ops::max2(CM[k], HGO[k]);
+        }
+      }
+      // Last row of a half: the end row and the corner.
+#pragma unroll
+      for (int h = 0; h < P; ++h) {
+        const int mh = h ? m1 : m0;
+        const int nh = h ? n1 : n0;
+        if (i == mh - 1) {
+          const uint32_t hm = Ops::half_mask(h);
+#pragma unroll
+          for (int k = 0; k < W; ++k) {
+            const int j = jbase + k;  // 0-based column
+            if (j < nh) {
+              uint32_t v = Ops::max2(acc.endrow, HGO[k]);
+              acc.endrow = (acc.endrow & ~hm) | (v & hm);
+            }
+            if (j == nh - 1) acc.corner = (acc.corner & ~hm) | (HGO[k] & hm);
+          }
+        }
+      }
+    }
+  }
+  if (track_endcol) {
+#pragma unroll
+    for (int h = 0; h < P; ++h) {
+      const int nh = h ? n1 : n0;
+      const uint32_t hm = Ops::half_mask(h);
+#pragma unroll
+      for (int k = 0; k < W; ++k)
+        if (jbase + k == nh - 1) acc.endcol = (acc.endcol & ~hm) | (CM[k] & hm);
+    }
+  }
+}
+
+// Max-reduce an accumulator word over the G lanes of a team.
+template <int G, int P>
+__device__ __forceinline__ uint32_t team_max(uint32_t v, unsigned wmask) {
+#pragma unroll
+  for (int off = G / 2; off > 0; off >>= 1) v = V<P>::max2(v, __shfl_xor_sync(wmask, v, off, G));
+  return v;
+}
+
+// Final score of half h from the team-reduced accumulators (HGO units: subtract go).
+template <int P>
+__device__ __forceinline__ int finish_score(const SchemeDev& S, const Acc& a, int h, bool* overflow) {
+  const int best = V<P>::get(a.best, h) - S.go;
+  if (P == 2) *overflow = best > S.ovf_limit;
+  if (S.mode == kModeLocal) return best;
+  const int corner = V<P>::get(a.corner, h) - S.go;
+  if (S.mode == kModeGlobal) return corner;
+  int res = corner;
+  if (S.free_q) res = max(res, V<P>::get(a.endcol, h) - S.go);
+  if (S.free_r) res = max(res, V<P>::get(a.endrow, h) - S.go);
+  if (S.free_q && S.free_r) res = max(res, 0);
+  return res;
+}
+
+}  // namespace gsw

@@ -1,0 +1,998 @@
+// Host side of the scoring engine: context, resident sequence sets, the length-binned
+// launch planner, the int16 -> int32 overflow rescoring and the C ABI of
+// include/gpusw_b200.h.
+#include <algorithm>
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/gpusw_b200.h"
+#include "kernels.cuh"
+
+namespace {
+
+using gsw::SchemeDev;
+
+struct Error {
+  int code;
+  std::string msg;
+};
+
+[[noreturn]] void fail(int code, const std::string& msg) { throw Error{code, msg}; }
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      fail(e_ == cudaErrorMemoryAllocation ? GPUSW_ERR_MEMORY : GPUSW_ERR_CUDA,           \
+           std::string(#call) + ": " + cudaGetErrorString(e_));                           \
+  } while (0)
+
+// Grow-only device buffer.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int64_t* held = nullptr;
+  void* get(size_t need) {
+    if (need > bytes) {
+      if (p) {
+        cudaFree(p);
+        if (held) *held -= (int64_t)bytes;
+      }
+      p = nullptr;
+      bytes = 0;
+      size_t want = std::max(need, bytes * 2);
+      CK(cudaMalloc(&p, want));
+      bytes = want;
+      if (held) *held += (int64_t)bytes;
+    }
+    return p;
+  }
+  template <class T> T* as(size_t n) { return static_cast<T*>(get(std::max<size_t>(1, n) * sizeof(T))); }
+  void release() {
+    if (p) cudaFree(p);
+    if (held && bytes) *held -= (int64_t)bytes;
+    p = nullptr;
+    bytes = 0;
+  }
+};
+
+struct Db {
+  int n = 0;
+  int bits = 2, per = 16, max_code = 0, max_len = 0;
+  std::vector<int> len;
+  std::vector<long long> woff;
+  std::vector<int> perm_desc;  // sequences by length, longest first (stable)
+  uint32_t* words = nullptr;
+  long long* woff_d = nullptr;
+  int* len_d = nullptr;
+  int* perm_d = nullptr;
+  int* ident_d = nullptr;      // identity order (plain form)
+  int64_t bytes = 0;
+  gsw::Packed packed() const {
+    gsw::Packed p;
+    p.words = words;
+    p.woff = woff_d;
+    p.len = len_d;
+    p.bits = bits;
+    p.per = per;
+    return p;
+  }
+};
+
+struct HostScheme {
+  int mode = 0, go = 0, ge = 0, free_q = 0, free_r = 0, ns = 0;
+  int max_sub = 0, min_sub = 0;
+  std::vector<int> sub;
+};
+
+// Kernel shapes compiled for the two kernels: team size G and columns per lane W.
+struct Shape {
+  int G, W;
+  int cap() const { return G * W; }
+};
+const Shape kCrossShapes[] = {{8, 8}, {16, 8}, {16, 16}, {32, 16}, {32, 32}};
+const Shape kPairShapes[] = {{8, 8}, {16, 8}, {16, 16}, {32, 16}};
+constexpr int kNumCross = sizeof(kCrossShapes) / sizeof(Shape);
+constexpr int kNumPair = sizeof(kPairShapes) / sizeof(Shape);
+constexpr size_t kSmemCap = 200 * 1024;
+constexpr int kOvfCap = 1 << 20;
+
+int pstride_of(const Shape& s) { return ((s.G * s.W / 4) + 7) & ~7; }
+size_t profile_bytes(const Shape& s, int ns) { return (size_t)(ns + 1) * pstride_of(s) * 16; }
+
+}  // namespace
+
+struct gpusw_ctx {
+  int device = 0;
+  int sms = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  bool has_scheme = false;
+  HostScheme sch;
+  int* sub_d = nullptr;
+  std::unordered_map<int, std::unique_ptr<Db>> dbs;
+  int next_db = 1;
+  int plain = 0;
+  int64_t mem_budget = 4ll << 30;
+  int64_t held = 0;
+  DevBuf out, meta, queue, ovf, ovf_count, bnd, topk_idx, topk_sc, flush;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
+  gpusw_stats st{};
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+void set_device(gpusw_ctx* c) { CK(cudaSetDevice(c->device)); }
+
+// ---------------------------------------------------------------------------- scheme
+SchemeDev make_scheme(const HostScheme& h, int P) {
+  SchemeDev S;
+  S.mode = h.mode;
+  S.free_q = h.free_q;
+  S.free_r = h.free_r;
+  S.go = h.go;
+  S.ge = h.ge;
+  S.ges = std::max(h.ge, h.go);
+  S.ns = h.ns;
+  S.pad_code = h.ns;
+  S.s_pad = std::min(0, h.min_sub);
+  const long long lo = P == 2 ? -32768ll : (long long)INT_MIN;
+  S.neg_low = (int)lo;
+  S.neg_f = (int)(lo - h.ge);
+  S.neg_e0 = (int)(lo - h.go);
+  S.ovf_limit = P == 2 ? 32767 - std::max(0, h.max_sub) : INT_MAX;
+  return S;
+}
+
+// Can every value of a DP of at most max_n columns and max_m rows be held in the width?
+// For int16 only the lower side is checked here; the upper side is caught at run time.
+bool width_ok(const HostScheme& h, int P, long long max_n, long long max_m) {
+  const long long lo = P == 2 ? -32768ll : (long long)INT_MIN;
+  const long long hi = P == 2 ? 32767ll : (long long)INT_MAX;
+  const long long g = std::min(h.go, h.ge);
+  const long long smin = std::min(0, h.min_sub);
+  const long long ges = std::max(h.ge, h.go);
+  const long long hmin = h.mode == gsw::kModeLocal ? 0 : (max_n + max_m) * g;
+  const long long lmin = hmin + 2 * g + smin;
+  if (lmin < lo + (ges - h.go)) return false;
+  if ((long long)h.max_sub - h.go > hi || smin - h.go < lo) return false;
+  if (P == 1) {
+    const long long hmax = std::min(max_n, max_m) * (long long)std::max(0, h.max_sub);
+    if (hmax + std::max(0, h.max_sub) > hi) return false;
+  }
+  return true;
+}
+
+// ------------------------------------------------------------------------- sequences
+void pack_host(const uint8_t* codes, const int32_t* offs, const Db& d, std::vector<uint32_t>& words) {
+  const int nthreads = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  auto work = [&](int t) {
+    for (int s = t; s < d.n; s += nthreads) {
+      const uint8_t* src = codes + offs[s];
+      const int len = d.len[s];
+      uint32_t* dst = words.data() + d.woff[s];
+      for (int c = 0; c < len; c += d.per) {
+        uint32_t v = 0;
+        const int e_end = std::min(d.per, len - c);
+        for (int e = 0; e < e_end; ++e) v |= (uint32_t)src[c + e] << (e * d.bits);
+        dst[c / d.per] = v;
+      }
+    }
+  };
+  if (d.n < 4096) {
+    for (int t = 0; t < nthreads; ++t) work(t);
+  } else {
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; ++t) th.emplace_back(work, t);
+    for (auto& x : th) x.join();
+  }
+}
+
+Db& get_db(gpusw_ctx* c, int32_t h) {
+  auto it = c->dbs.find(h);
+  if (it == c->dbs.end()) fail(GPUSW_ERR_NOT_FOUND, "unknown sequence-set handle " + std::to_string(h));
+  return *it->second;
+}
+
+void require_scheme(gpusw_ctx* c, const Db& a, const Db& b) {
+  if (!c->has_scheme) fail(GPUSW_ERR_SCHEME, "no scheme set (call gpusw_set_scheme first)");
+  if (a.max_code >= c->sch.ns || b.max_code >= c->sch.ns)
+    fail(GPUSW_ERR_INVALID, "sequence codes exceed the scheme's substitution table");
+}
+
+// -------------------------------------------------------------------------- launches
+template <int G, int W, int P, bool L>
+void launch_cross_t(gpusw_ctx* c, const gsw::CrossParams& prm, size_t smem) {
+  auto k = gsw::cross_kernel<G, W, P, L>;
+  static int configured_dev = -1;
+  static int blocks_per_sm = 1;
+  static size_t configured_smem = 0;
+  if (configured_dev != c->device || configured_smem < smem) {
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(smem, configured_smem)));
+    configured_smem = std::max(smem, configured_smem);
+    configured_dev = c->device;
+  }
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k, 256, smem));
+  int grid = c->sms * std::max(1, blocks_per_sm);
+  grid = (int)std::min<long long>(grid, std::max(1, prm.n_items));
+  k<<<grid, 256, smem, c->stream>>>(prm);
+  CK(cudaGetLastError());
+  c->st.last_launches++;
+}
+
+template <int P, bool L>
+void launch_cross_shape(gpusw_ctx* c, int shape, const gsw::CrossParams& prm, size_t smem) {
+  switch (shape) {
+    case 0: launch_cross_t<8, 8, P, L>(c, prm, smem); break;
+    case 1: launch_cross_t<16, 8, P, L>(c, prm, smem); break;
+    case 2: launch_cross_t<16, 16, P, L>(c, prm, smem); break;
+    case 3: launch_cross_t<32, 16, P, L>(c, prm, smem); break;
+    case 4: launch_cross_t<32, 32, P, L>(c, prm, smem); break;
+    default: fail(GPUSW_ERR_INVALID, "bad cross kernel shape");
+  }
+}
+
+void launch_cross(gpusw_ctx* c, int shape, int P, bool local, const gsw::CrossParams& prm, size_t smem) {
+  if (P == 2) {
+    if (local) launch_cross_shape<2, true>(c, shape, prm, smem);
+    else launch_cross_shape<2, false>(c, shape, prm, smem);
+  } else {
+    if (local) launch_cross_shape<1, true>(c, shape, prm, smem);
+    else launch_cross_shape<1, false>(c, shape, prm, smem);
+  }
+}
+
+// Teams per CTA of the pairs kernel: each team holds its own profile.
+int pair_teams(const Shape& s, int ns) {
+  const int t = (int)std::min<size_t>(256 / s.G, kSmemCap / profile_bytes(s, ns));
+  return std::max(1, t);
+}
+
+template <int G, int W, int P, bool L>
+void launch_pairs_t(gpusw_ctx* c, gsw::PairsParams prm, int teams, long long max_rows, bool multipass) {
+  auto k = gsw::pairs_kernel<G, W, P, L>;
+  const Shape s{G, W};
+  const size_t smem = profile_bytes(s, prm.S.ns) * teams;
+  static int configured_dev = -1;
+  static size_t configured_smem = 0;
+  if (configured_dev != c->device || configured_smem < smem) {
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(smem, configured_smem)));
+    configured_smem = std::max(smem, configured_smem);
+    configured_dev = c->device;
+  }
+  int bps = 1;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, G * teams, smem));
+  long long grid = (long long)c->sms * std::max(1, bps);
+  const long long team_items = prm.item_mode == 1 ? kOvfCap : prm.n_items;
+  grid = std::max(1ll, std::min(grid, (team_items + teams - 1) / teams));
+  if (multipass) {
+    const size_t need = (size_t)grid * teams * (size_t)std::max(1ll, max_rows) * sizeof(uint2);
+    prm.bnd = c->bnd.as<uint2>(need / sizeof(uint2));
+    prm.bnd_cap = (int)std::max(1ll, max_rows);
+  } else {
+    prm.bnd = nullptr;
+    prm.bnd_cap = 0;
+  }
+  k<<<(int)grid, G * teams, smem, c->stream>>>(prm);
+  CK(cudaGetLastError());
+  c->st.last_launches++;
+}
+
+template <int P, bool L>
+void launch_pairs_shape(gpusw_ctx* c, int shape, const gsw::PairsParams& prm, int teams, long long max_rows, bool mp) {
+  switch (shape) {
+    case 0: launch_pairs_t<8, 8, P, L>(c, prm, teams, max_rows, mp); break;
+    case 1: launch_pairs_t<16, 8, P, L>(c, prm, teams, max_rows, mp); break;
+    case 2: launch_pairs_t<16, 16, P, L>(c, prm, teams, max_rows, mp); break;
+    case 3: launch_pairs_t<32, 16, P, L>(c, prm, teams, max_rows, mp); break;
+    default: fail(GPUSW_ERR_INVALID, "bad pairs kernel shape");
+  }
+}
+
+void launch_pairs(gpusw_ctx* c, int shape, int P, bool local, const gsw::PairsParams& prm,
+                  long long max_rows, bool multipass) {
+  const int teams = pair_teams(kPairShapes[shape], prm.S.ns);
+  if (P == 2) {
+    if (local) launch_pairs_shape<2, true>(c, shape, prm, teams, max_rows, multipass);
+    else launch_pairs_shape<2, false>(c, shape, prm, teams, max_rows, multipass);
+  } else {
+    if (local) launch_pairs_shape<1, true>(c, shape, prm, teams, max_rows, multipass);
+    else launch_pairs_shape<1, false>(c, shape, prm, teams, max_rows, multipass);
+  }
+}
+
+// Smallest compiled shape whose columns cover `ncols` and whose profile fits; -1 if none.
+int pick_cross_shape(int ncols, int ns) {
+  for (int i = 0; i < kNumCross; ++i)
+    if (kCrossShapes[i].cap() >= ncols && profile_bytes(kCrossShapes[i], ns) <= kSmemCap) return i;
+  return -1;
+}
+int pick_pair_shape(int ncols, int ns) {
+  for (int i = 0; i < kNumPair; ++i)
+    if (kPairShapes[i].cap() >= ncols && profile_bytes(kPairShapes[i], ns) <= kSmemCap) return i;
+  for (int i = kNumPair - 1; i >= 0; --i)  // multi-pass: the widest shape that fits
+    if (profile_bytes(kPairShapes[i], ns) <= kSmemCap) return i;
+  return 0;
+}
+
+// Host staging of several arrays into one device allocation.
+struct Staging {
+  std::vector<char> host;
+  size_t add(const void* src, size_t bytes) {
+    size_t off = (host.size() + 255) & ~(size_t)255;
+    host.resize(off + bytes);
+    if (bytes) memcpy(host.data() + off, src, bytes);
+    return off;
+  }
+  char* upload(gpusw_ctx* c) {
+    char* d = static_cast<char*>(c->meta.get(std::max<size_t>(host.size(), 256)));
+    if (!host.empty()) CK(cudaMemcpyAsync(d, host.data(), host.size(), cudaMemcpyHostToDevice, c->stream));
+    return d;
+  }
+};
+
+// Overflow rescoring of the int16 cells flagged by the previous launches (int32, any length).
+void launch_overflow_rescore(gpusw_ctx* c, const Db& q, const Db& r, int* out,
+                             unsigned long long* queue_slot) {
+  gsw::PairsParams pp{};
+  pp.S = make_scheme(c->sch, 1);
+  pp.sub = c->sub_d;
+  pp.cols = q.packed();
+  pp.rows = r.packed();
+  pp.item_mode = 1;
+  pp.ovf_in = static_cast<const gsw::Ovf*>(c->ovf.p);
+  pp.ovf_in_count = static_cast<const int*>(c->ovf_count.p);
+  pp.ovf_in_cap = kOvfCap;
+  pp.queue = queue_slot;
+  pp.out = out;
+  pp.n_items = kOvfCap;
+  const int shape = pick_pair_shape(1 << 30, c->sch.ns);
+  launch_pairs(c, shape, 1, c->sch.mode == gsw::kModeLocal, pp, std::max(q.max_len, r.max_len), true);
+}
+
+// Cross product of the queries `qlist` (a sublist of q) against every sequence of r into
+// out[a * out_ld + ref] for a = position in qlist. P = 2 (int16 pairs) or 1 (int32).
+// Returns the number of queue counters used (device slots at queues[...]).
+void run_cross(gpusw_ctx* c, const Db& q, const Db& r, const int32_t* qlist, int nq, int P,
+               int* out, long long out_ld) {
+  const HostScheme& h = c->sch;
+  const bool local = h.mode == gsw::kModeLocal;
+  const int nr = r.n;
+  if (nq == 0 || nr == 0) return;
+  // column order: longest first (batched) or input order (plain)
+  std::vector<int> pos(nq);
+  std::iota(pos.begin(), pos.end(), 0);
+  if (!c->plain)
+    std::stable_sort(pos.begin(), pos.end(), [&](int a, int b) { return q.len[qlist[a]] > q.len[qlist[b]]; });
+  // column pairs (P = 2) or singles (P = 1)
+  const int npairs = (nq + P - 1) / P;
+  std::vector<int2> pairs(npairs), pair_out(npairs);
+  std::vector<int> pair_cols(npairs);
+  for (int i = 0; i < npairs; ++i) {
+    const int a = pos[i * P];
+    const int b = (P == 2 && i * P + 1 < nq) ? pos[i * P + 1] : -1;
+    pairs[i] = make_int2(qlist[a], b >= 0 ? qlist[b] : -1);
+    pair_out[i] = make_int2(a, b);
+    pair_cols[i] = std::max(q.len[qlist[a]], b >= 0 ? q.len[qlist[b]] : 0);
+  }
+  // bins by kernel shape; columns longer than any shape go to the multi-pass pairs kernel
+  int plain_shape = -2;
+  if (c->plain) {
+    const int mx = *std::max_element(pair_cols.begin(), pair_cols.end());
+    plain_shape = pick_cross_shape(std::max(1, mx), h.ns);
+  }
+  std::vector<std::vector<int>> bins(kNumCross);
+  std::vector<int> longp;
+  for (int i = 0; i < npairs; ++i) {
+    const int s = c->plain ? plain_shape : pick_cross_shape(std::max(1, pair_cols[i]), h.ns);
+    if (s < 0) longp.push_back(i);
+    else bins[s].push_back(i);
+  }
+  // rows: longest first (batched) or input order (plain); chunks of rows per work item
+  const int* row_perm_d = c->plain ? r.ident_d : r.perm_d;
+  const std::vector<int>* row_order = &r.perm_desc;
+  std::vector<int> ident;
+  if (c->plain) {
+    ident.resize(nr);
+    std::iota(ident.begin(), ident.end(), 0);
+    row_order = &ident;
+  }
+  Staging stg;
+  const size_t off_pairs = stg.add(pairs.data(), pairs.size() * sizeof(int2));
+  const size_t off_pout = stg.add(pair_out.data(), pair_out.size() * sizeof(int2));
+  struct Launch { int shape; size_t items_off; int n_items; int rows_per_item; };
+  std::vector<Launch> launches;
+  for (int s = 0; s < kNumCross; ++s) {
+    if (bins[s].empty()) continue;
+    const int teams = 256 / kCrossShapes[s].G;
+    const int rpi = c->plain ? teams * 2 : teams * 4;
+    const int nchunks = (nr + rpi - 1) / rpi;
+    // chunk cost: rows are sorted, so chunk order is already costliest first
+    std::vector<int2> items;
+    items.reserve((size_t)nchunks * bins[s].size());
+    for (int ch = 0; ch < nchunks; ++ch)
+      for (int pi : bins[s]) items.push_back(make_int2(pi, ch));
+    launches.push_back({s, stg.add(items.data(), items.size() * sizeof(int2)), (int)items.size(), rpi});
+  }
+  std::vector<int2> long_pairs, long_pout;
+  size_t off_lp = 0, off_lpo = 0;
+  for (int i : longp) { long_pairs.push_back(pairs[i]); long_pout.push_back(pair_out[i]); }
+  if (!longp.empty()) {
+    off_lp = stg.add(long_pairs.data(), long_pairs.size() * sizeof(int2));
+    off_lpo = stg.add(long_pout.data(), long_pout.size() * sizeof(int2));
+  }
+  char* dmeta = stg.upload(c);
+  const int nq_slots = (int)launches.size() + 2;
+  unsigned long long* queues = c->queue.as<unsigned long long>(nq_slots);
+  CK(cudaMemsetAsync(queues, 0, nq_slots * sizeof(unsigned long long), c->stream));
+  if (P == 2) CK(cudaMemsetAsync(c->ovf_count.as<int>(1), 0, sizeof(int), c->stream));
+  gsw::CrossParams cp{};
+  cp.S = make_scheme(h, P);
+  cp.sub = c->sub_d;
+  cp.cols = q.packed();
+  cp.rows = r.packed();
+  cp.pairs = reinterpret_cast<const int2*>(dmeta + off_pairs);
+  cp.pair_out = reinterpret_cast<const int2*>(dmeta + off_pout);
+  cp.row_perm = row_perm_d;
+  cp.n_rows = nr;
+  cp.out = out;
+  cp.out_ld = out_ld;
+  cp.ovf = c->ovf.as<gsw::Ovf>(kOvfCap);
+  cp.ovf_count = c->ovf_count.as<int>(1);
+  cp.ovf_cap = kOvfCap;
+  int slot = 0;
+  for (const Launch& L : launches) {
+    cp.items = reinterpret_cast<const int2*>(dmeta + L.items_off);
+    cp.n_items = L.n_items;
+    cp.rows_per_item = L.rows_per_item;
+    cp.queue = reinterpret_cast<int*>(queues + slot++);
+    launch_cross(c, L.shape, P, local, cp, profile_bytes(kCrossShapes[L.shape], h.ns));
+  }
+  if (!longp.empty()) {
+    gsw::PairsParams pp{};
+    pp.S = cp.S;
+    pp.sub = c->sub_d;
+    pp.cols = cp.cols;
+    pp.rows = cp.rows;
+    pp.item_mode = 2;
+    pp.pairs = reinterpret_cast<const int2*>(dmeta + off_lp);
+    pp.pair_out = reinterpret_cast<const int2*>(dmeta + off_lpo);
+    pp.row_perm = r.perm_d;
+    pp.n_rows = nr;
+    pp.out_ld = out_ld;
+    pp.n_items = (long long)longp.size() * nr;
+    pp.queue = queues + slot++;
+    pp.out = out;
+    pp.ovf = cp.ovf;
+    pp.ovf_count = cp.ovf_count;
+    pp.ovf_cap = kOvfCap;
+    launch_pairs(c, pick_pair_shape(1 << 30, h.ns), P, local, pp, r.max_len, true);
+  }
+  if (P == 2) launch_overflow_rescore(c, q, r, out, queues + slot++);
+  (void)row_order;
+}
+
+int read_overflow_count(gpusw_ctx* c) {
+  int n = 0;
+  CK(cudaMemcpyAsync(&n, c->ovf_count.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return n;
+}
+
+int choose_width(gpusw_ctx* c, int dtype, int max_n, int max_m) {
+  if (!width_ok(c->sch, 1, max_n, max_m))
+    fail(GPUSW_ERR_OVERFLOW, "scores of this scheme and these lengths do not fit in int32");
+  if (dtype == GPUSW_DTYPE_INT32) return 1;
+  return width_ok(c->sch, 2, max_n, max_m) ? 2 : 1;
+}
+
+void begin_call(gpusw_ctx* c) {
+  set_device(c);
+  c->st.last_launches = 0;
+  c->st.last_overflow = 0;
+  c->st.last_pairs = 0;
+  c->st.last_cells = 0;
+  CK(cudaEventRecord(c->ev0, c->stream));
+}
+
+void end_call(gpusw_ctx* c) {
+  CK(cudaEventSynchronize(c->ev3));
+  float k = 0, t = 0;
+  CK(cudaEventElapsedTime(&k, c->ev1, c->ev2));
+  CK(cudaEventElapsedTime(&t, c->ev0, c->ev3));
+  c->st.last_kernel_ms = k;
+  c->st.last_total_ms = t;
+  c->st.total_launches += c->st.last_launches;
+  c->st.total_overflow += c->st.last_overflow;
+  c->st.device_bytes = c->held;
+}
+
+template <class F>
+int guarded(gpusw_ctx* c, F&& f) {
+  if (!c) return GPUSW_ERR_INVALID;
+  try {
+    f();
+    return GPUSW_OK;
+  } catch (const Error& e) {
+    c->err = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    c->err = "host allocation failed";
+    return GPUSW_ERR_MEMORY;
+  } catch (const std::exception& e) {
+    c->err = e.what();
+    return GPUSW_ERR_CUDA;
+  }
+}
+
+__global__ void dpx_rate_kernel(const unsigned* in, unsigned* out, int iters) {
+  unsigned x[8], cst[8];
+  const unsigned b = in[0];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    x[k] = in[1 + k] + threadIdx.x;
+    cst[k] = in[1 + (k & 3)] ^ (threadIdx.x << 3);
+  }
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = __viaddmax_s16x2(x[k], b, cst[k]);
+  }
+  unsigned acc = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc ^= x[k];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = acc;
+}
+
+}  // namespace
+
+// ================================================================================ C ABI
+extern "C" {
+
+int gpusw_version(void) { return 100; }
+
+int gpusw_device_count(int* count) {
+  if (!count) return GPUSW_ERR_INVALID;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    n = 0;
+  }
+  *count = n;
+  return GPUSW_OK;
+}
+
+int gpusw_ctx_create(int device, gpusw_ctx** out) {
+  if (!out) return GPUSW_ERR_INVALID;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    g_create_error = "no CUDA device is available";
+    return GPUSW_ERR_NO_GPU;
+  }
+  if (device < 0 || device >= n) {
+    g_create_error = "device ordinal out of range";
+    return GPUSW_ERR_INVALID;
+  }
+  auto* c = new gpusw_ctx();
+  c->device = device;
+  for (DevBuf* b : {&c->out, &c->meta, &c->queue, &c->ovf, &c->ovf_count, &c->bnd, &c->topk_idx,
+                    &c->topk_sc, &c->flush})
+    b->held = &c->held;
+  int rc = guarded(c, [&] {
+    set_device(c);
+    CK(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&c->ev0, &c->ev1, &c->ev2, &c->ev3}) CK(cudaEventCreate(e));
+  });
+  if (rc != GPUSW_OK) {
+    g_create_error = c->err;
+    gpusw_ctx_destroy(c);
+    return rc;
+  }
+  *out = c;
+  return GPUSW_OK;
+}
+
+void gpusw_ctx_destroy(gpusw_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto& kv : c->dbs) {
+    Db& d = *kv.second;
+    cudaFree(d.words);
+    cudaFree(d.woff_d);
+    cudaFree(d.len_d);
+    cudaFree(d.perm_d);
+    cudaFree(d.ident_d);
+  }
+  for (DevBuf* b : {&c->out, &c->meta, &c->queue, &c->ovf, &c->ovf_count, &c->bnd, &c->topk_idx,
+                    &c->topk_sc, &c->flush})
+    b->release();
+  if (c->sub_d) cudaFree(c->sub_d);
+  for (cudaEvent_t e : {c->ev0, c->ev1, c->ev2, c->ev3})
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char* gpusw_last_error(const gpusw_ctx* c) {
+  return c ? c->err.c_str() : g_create_error.c_str();
+}
+
+int gpusw_set_scheme(gpusw_ctx* c, int mode, int go, int ge, int free_q, int free_r, int ns,
+                     const int32_t* sub) {
+  return guarded(c, [&] {
+    if (mode < 0 || mode > 2) fail(GPUSW_ERR_SCHEME, "mode must be 0 (local), 1 (global) or 2 (semiglobal)");
+    if (go > 0 || ge > 0) fail(GPUSW_ERR_SCHEME, "gap_open and gap_extend must be <= 0");
+    if (ns < 2 || ns > 256) fail(GPUSW_ERR_SCHEME, "substitution table side must be in [2, 256]");
+    if (!sub) fail(GPUSW_ERR_INVALID, "null substitution table");
+    if (go < -(1 << 24) || ge < -(1 << 24)) fail(GPUSW_ERR_SCHEME, "gap costs below -2^24 are not supported");
+    HostScheme h;
+    h.mode = mode;
+    h.go = go;
+    h.ge = ge;
+    h.free_q = free_q ? 1 : 0;
+    h.free_r = free_r ? 1 : 0;
+    h.ns = ns;
+    h.sub.assign(sub, sub + (size_t)ns * ns);
+    h.max_sub = *std::max_element(h.sub.begin(), h.sub.end());
+    h.min_sub = *std::min_element(h.sub.begin(), h.sub.end());
+    if (h.max_sub > (1 << 24) || h.min_sub < -(1 << 24))
+      fail(GPUSW_ERR_SCHEME, "substitution scores beyond +/-2^24 are not supported");
+    set_device(c);
+    if (c->sub_d) cudaFree(c->sub_d);
+    c->sub_d = nullptr;
+    CK(cudaMalloc(&c->sub_d, h.sub.size() * sizeof(int)));
+    CK(cudaMemcpy(c->sub_d, h.sub.data(), h.sub.size() * sizeof(int), cudaMemcpyHostToDevice));
+    c->sch = std::move(h);
+    c->has_scheme = true;
+  });
+}
+
+int gpusw_db_upload(gpusw_ctx* c, const uint8_t* codes, const int32_t* offsets, int32_t n, int32_t* out_db) {
+  return guarded(c, [&] {
+    if (!offsets || !out_db || n < 0) fail(GPUSW_ERR_INVALID, "null offsets/handle or negative count");
+    if (offsets[0] < 0) fail(GPUSW_ERR_INVALID, "offsets must be non-negative");
+    for (int i = 0; i < n; ++i)
+      if (offsets[i + 1] < offsets[i]) fail(GPUSW_ERR_INVALID, "offsets must be non-decreasing");
+    const long long total = n ? (long long)offsets[n] - offsets[0] : 0;
+    if (total > 0 && !codes) fail(GPUSW_ERR_INVALID, "null codes");
+    auto d = std::make_unique<Db>();
+    d->n = n;
+    d->len.resize(n);
+    int maxc = 0;
+    for (int i = 0; i < n; ++i) {
+      d->len[i] = offsets[i + 1] - offsets[i];
+      d->max_len = std::max(d->max_len, d->len[i]);
+    }
+    if (n) {
+      const uint8_t* b = codes + offsets[0];
+      for (long long k = 0; k < total; ++k) maxc = std::max<int>(maxc, b[k]);
+    }
+    d->max_code = maxc;
+    d->bits = maxc < 4 ? 2 : maxc < 16 ? 4 : maxc < 32 ? 5 : 8;
+    d->per = d->bits == 5 ? 6 : 32 / d->bits;
+    d->woff.resize(n);
+    long long w = 0;
+    for (int i = 0; i < n; ++i) {
+      d->woff[i] = w;
+      w += ((d->len[i] + d->per - 1) / d->per + 3) & ~3ll;
+    }
+    const long long nwords = w + 64;  // tail slack for read-ahead
+    std::vector<uint32_t> words((size_t)nwords, 0u);
+    // offsets are relative to codes[0] in the ABI (like the reference's Encoded)
+    pack_host(codes, offsets, *d, words);
+    d->perm_desc.resize(n);
+    std::iota(d->perm_desc.begin(), d->perm_desc.end(), 0);
+    std::stable_sort(d->perm_desc.begin(), d->perm_desc.end(),
+                     [&](int a, int b) { return d->len[a] > d->len[b]; });
+    std::vector<int> ident(n);
+    std::iota(ident.begin(), ident.end(), 0);
+    set_device(c);
+    CK(cudaMalloc(&d->words, nwords * sizeof(uint32_t)));
+    CK(cudaMalloc(&d->woff_d, std::max(1, n) * sizeof(long long)));
+    CK(cudaMalloc(&d->len_d, std::max(1, n) * sizeof(int)));
+    CK(cudaMalloc(&d->perm_d, std::max(1, n) * sizeof(int)));
+    CK(cudaMalloc(&d->ident_d, std::max(1, n) * sizeof(int)));
+    d->bytes = nwords * 4 + (long long)std::max(1, n) * 20;
+    CK(cudaMemcpyAsync(d->words, words.data(), nwords * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+    if (n) {
+      CK(cudaMemcpyAsync(d->woff_d, d->woff.data(), n * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemcpyAsync(d->len_d, d->len.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemcpyAsync(d->perm_d, d->perm_desc.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemcpyAsync(d->ident_d, ident.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    c->held += d->bytes;
+    const int h = c->next_db++;
+    c->dbs[h] = std::move(d);
+    *out_db = h;
+  });
+}
+
+int gpusw_db_free(gpusw_ctx* c, int32_t db) {
+  return guarded(c, [&] {
+    Db& d = get_db(c, db);
+    set_device(c);
+    CK(cudaStreamSynchronize(c->stream));
+    cudaFree(d.words);
+    cudaFree(d.woff_d);
+    cudaFree(d.len_d);
+    cudaFree(d.perm_d);
+    cudaFree(d.ident_d);
+    c->held -= d.bytes;
+    c->dbs.erase(db);
+  });
+}
+
+int gpusw_db_bits(gpusw_ctx* c, int32_t db) {
+  int bits = 0;
+  int rc = guarded(c, [&] { bits = get_db(c, db).bits; });
+  return rc == GPUSW_OK ? bits : -rc;
+}
+
+int gpusw_score_cross(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qlist, int32_t nq,
+                      int dtype, int32_t* out) {
+  return guarded(c, [&] {
+    Db& q = get_db(c, qdb);
+    Db& r = get_db(c, rdb);
+    require_scheme(c, q, r);
+    if (nq < 0 || (nq > 0 && (!qlist || !out))) fail(GPUSW_ERR_INVALID, "null qlist/out");
+    int max_n = 0;
+    double qsum = 0;
+    for (int a = 0; a < nq; ++a) {
+      if (qlist[a] < 0 || qlist[a] >= q.n) fail(GPUSW_ERR_INVALID, "query index out of range");
+      max_n = std::max(max_n, q.len[qlist[a]]);
+      qsum += q.len[qlist[a]];
+    }
+    begin_call(c);
+    const long long total = (long long)nq * r.n;
+    int P = choose_width(c, dtype, max_n, r.max_len);
+    int* d_out = c->out.as<int>(total);
+    CK(cudaEventRecord(c->ev1, c->stream));
+    run_cross(c, q, r, qlist, nq, P, d_out, r.n);
+    CK(cudaEventRecord(c->ev2, c->stream));
+    if (P == 2 && total > 0) {
+      const int n_ovf = read_overflow_count(c);
+      c->st.last_overflow = n_ovf;
+      if (n_ovf > kOvfCap) {  // too many to rescore one by one: redo everything in int32
+        CK(cudaEventRecord(c->ev1, c->stream));
+        run_cross(c, q, r, qlist, nq, 1, d_out, r.n);
+        CK(cudaEventRecord(c->ev2, c->stream));
+      }
+    }
+    if (total > 0) CK(cudaMemcpyAsync(out, d_out, total * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaEventRecord(c->ev3, c->stream));
+    double rsum = 0;
+    for (int l : r.len) rsum += l;
+    c->st.last_cells = qsum * rsum;
+    c->st.last_pairs = total;
+    end_call(c);
+  });
+}
+
+int gpusw_topk(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qlist, int32_t nq, int32_t k,
+               int dtype, int32_t* out_idx, int32_t* out_score) {
+  return guarded(c, [&] {
+    Db& q = get_db(c, qdb);
+    Db& r = get_db(c, rdb);
+    require_scheme(c, q, r);
+    if (k < 0) fail(GPUSW_ERR_INVALID, "k must be >= 0");
+    if (nq < 0 || (nq > 0 && !qlist)) fail(GPUSW_ERR_INVALID, "null qlist");
+    const int kk = std::min(k, r.n);
+    if (nq > 0 && kk > 0 && (!out_idx || !out_score)) fail(GPUSW_ERR_INVALID, "null outputs");
+    int max_n = 0;
+    double qsum = 0;
+    for (int a = 0; a < nq; ++a) {
+      if (qlist[a] < 0 || qlist[a] >= q.n) fail(GPUSW_ERR_INVALID, "query index out of range");
+      max_n = std::max(max_n, q.len[qlist[a]]);
+      qsum += q.len[qlist[a]];
+    }
+    begin_call(c);
+    CK(cudaEventRecord(c->ev1, c->stream));
+    if (nq > 0 && kk > 0) {
+      const int P = choose_width(c, dtype, max_n, r.max_len);
+      const long long row_bytes = (long long)r.n * 4;
+      int qb = (int)std::max(1ll, std::min<long long>(nq, c->mem_budget / std::max(1ll, row_bytes)));
+      if (c->plain) qb = std::min(qb, 16);
+      int* d_out = c->out.as<int>((size_t)qb * r.n);
+      int* d_idx = c->topk_idx.as<int>((size_t)nq * kk);
+      int* d_sc = c->topk_sc.as<int>((size_t)nq * kk);
+      for (int b0 = 0; b0 < nq; b0 += qb) {
+        const int nb = std::min(qb, nq - b0);
+        run_cross(c, q, r, qlist + b0, nb, P, d_out, r.n);
+        if (P == 2) {
+          const int n_ovf = read_overflow_count(c);
+          c->st.last_overflow += n_ovf;
+          if (n_ovf > kOvfCap) run_cross(c, q, r, qlist + b0, nb, 1, d_out, r.n);
+        }
+        gsw::topk_kernel<<<nb, 256, 0, c->stream>>>(d_out, r.n, r.n, kk, d_idx + (size_t)b0 * kk,
+                                                     d_sc + (size_t)b0 * kk, kk);
+        CK(cudaGetLastError());
+        c->st.last_launches++;
+        if (c->plain) {
+          CK(cudaMemcpyAsync(out_idx + (size_t)b0 * kk, d_idx + (size_t)b0 * kk, (size_t)nb * kk * 4, cudaMemcpyDeviceToHost, c->stream));
+          CK(cudaMemcpyAsync(out_score + (size_t)b0 * kk, d_sc + (size_t)b0 * kk, (size_t)nb * kk * 4, cudaMemcpyDeviceToHost, c->stream));
+          CK(cudaStreamSynchronize(c->stream));
+        }
+      }
+      CK(cudaEventRecord(c->ev2, c->stream));
+      if (!c->plain) {
+        CK(cudaMemcpyAsync(out_idx, d_idx, (size_t)nq * kk * 4, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(out_score, d_sc, (size_t)nq * kk * 4, cudaMemcpyDeviceToHost, c->stream));
+      }
+    } else {
+      CK(cudaEventRecord(c->ev2, c->stream));
+    }
+    CK(cudaEventRecord(c->ev3, c->stream));
+    double rsum = 0;
+    for (int l : r.len) rsum += l;
+    c->st.last_cells = qsum * rsum;
+    c->st.last_pairs = (long long)nq * r.n;
+    end_call(c);
+  });
+}
+
+int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi, const int32_t* rj,
+                      int64_t n, int dtype, int32_t* out) {
+  return guarded(c, [&] {
+    Db& q = get_db(c, qdb);
+    Db& r = get_db(c, rdb);
+    require_scheme(c, q, r);
+    if (n < 0 || (n > 0 && (!qi || !rj || !out))) fail(GPUSW_ERR_INVALID, "null pair arrays");
+    if (n >= (1ll << 31)) fail(GPUSW_ERR_INVALID, "at most 2^31 - 1 pairs per call");
+    int max_n = 0, max_m = 0;
+    double cells = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      if (qi[i] < 0 || qi[i] >= q.n || rj[i] < 0 || rj[i] >= r.n)
+        fail(GPUSW_ERR_INVALID, "pair index out of range at position " + std::to_string(i));
+      max_n = std::max(max_n, q.len[qi[i]]);
+      max_m = std::max(max_m, r.len[rj[i]]);
+      cells += (double)q.len[qi[i]] * r.len[rj[i]];
+    }
+    begin_call(c);
+    CK(cudaEventRecord(c->ev1, c->stream));
+    const HostScheme& h = c->sch;
+    const bool local = h.mode == gsw::kModeLocal;
+    int P = n > 0 ? choose_width(c, dtype, max_n, max_m) : 1;
+    int* d_out = c->out.as<int>((size_t)std::max<int64_t>(1, n));
+    auto run = [&](int Pw) {
+      // order: by kernel shape (column length), then row length, then column length
+      std::vector<int> order((size_t)n);
+      std::iota(order.begin(), order.end(), 0);
+      std::vector<int> shp((size_t)n);
+      int plain_shape = 0;
+      if (c->plain) plain_shape = pick_pair_shape(std::max(1, max_n), h.ns);
+      for (int64_t i = 0; i < n; ++i) shp[i] = c->plain ? plain_shape : pick_pair_shape(std::max(1, q.len[qi[i]]), h.ns);
+      if (!c->plain)
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+          if (shp[a] != shp[b]) return shp[a] < shp[b];
+          const int ma = r.len[rj[a]], mb = r.len[rj[b]];
+          if (ma != mb) return ma > mb;
+          return q.len[qi[a]] > q.len[qi[b]];
+        });
+      Staging stg;
+      const size_t o_qi = stg.add(qi, (size_t)n * 4), o_rj = stg.add(rj, (size_t)n * 4);
+      const size_t o_ord = stg.add(order.data(), (size_t)n * 4);
+      char* dm = stg.upload(c);
+      const int nslots = kNumPair + 2;
+      unsigned long long* queues = c->queue.as<unsigned long long>(nslots);
+      CK(cudaMemsetAsync(queues, 0, nslots * sizeof(unsigned long long), c->stream));
+      if (Pw == 2) CK(cudaMemsetAsync(c->ovf_count.as<int>(1), 0, sizeof(int), c->stream));
+      gsw::PairsParams pp{};
+      pp.S = make_scheme(h, Pw);
+      pp.sub = c->sub_d;
+      pp.cols = q.packed();
+      pp.rows = r.packed();
+      pp.qi = reinterpret_cast<const int*>(dm + o_qi);
+      pp.rj = reinterpret_cast<const int*>(dm + o_rj);
+      pp.item_mode = 0;
+      pp.out = d_out;
+      pp.ovf = c->ovf.as<gsw::Ovf>(kOvfCap);
+      pp.ovf_count = c->ovf_count.as<int>(1);
+      pp.ovf_cap = kOvfCap;
+      int64_t i0 = 0;
+      int slot = 0;
+      while (i0 < n) {
+        const int s = shp[order[i0]];
+        int64_t i1 = i0;
+        int mrow = 0, mcol = 0;
+        while (i1 < n && shp[order[i1]] == s) {
+          mrow = std::max(mrow, r.len[rj[order[i1]]]);
+          mcol = std::max(mcol, q.len[qi[order[i1]]]);
+          ++i1;
+        }
+        pp.order = reinterpret_cast<const int*>(dm + o_ord) + i0;
+        pp.n_align = i1 - i0;
+        pp.n_items = (pp.n_align + Pw - 1) / Pw;
+        pp.queue = queues + slot++;
+        launch_pairs(c, s, Pw, local, pp, mrow, mcol > kPairShapes[s].cap());
+        i0 = i1;
+      }
+      if (Pw == 2) launch_overflow_rescore(c, q, r, d_out, queues + slot++);
+    };
+    if (n > 0) {
+      run(P);
+      if (P == 2) {
+        const int n_ovf = read_overflow_count(c);
+        c->st.last_overflow = n_ovf;
+        if (n_ovf > kOvfCap) run(1);
+      }
+    }
+    CK(cudaEventRecord(c->ev2, c->stream));
+    if (n > 0) CK(cudaMemcpyAsync(out, d_out, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaEventRecord(c->ev3, c->stream));
+    c->st.last_cells = cells;
+    c->st.last_pairs = n;
+    end_call(c);
+  });
+}
+
+int gpusw_set_options(gpusw_ctx* c, int plain, int64_t mem_budget) {
+  return guarded(c, [&] {
+    if (mem_budget < 0) fail(GPUSW_ERR_INVALID, "negative memory budget");
+    c->plain = plain ? 1 : 0;
+    c->mem_budget = mem_budget ? mem_budget : (4ll << 30);
+  });
+}
+
+int gpusw_get_stats(gpusw_ctx* c, gpusw_stats* out) {
+  return guarded(c, [&] {
+    if (!out) fail(GPUSW_ERR_INVALID, "null stats");
+    c->st.device_bytes = c->held;
+    *out = c->st;
+  });
+}
+
+int gpusw_sync(gpusw_ctx* c) {
+  return guarded(c, [&] {
+    set_device(c);
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int gpusw_measure_dpx_rate(gpusw_ctx* c, double* ops_per_s) {
+  return guarded(c, [&] {
+    if (!ops_per_s) fail(GPUSW_ERR_INVALID, "null output");
+    set_device(c);
+    const int blocks = c->sms * 8, threads = 256, iters = 4096;
+    unsigned hin[16];
+    for (int i = 0; i < 16; ++i) hin[i] = 0x00030005u * (i + 1);
+    hin[0] = 0xFFFEFFFEu;
+    unsigned* din = static_cast<unsigned*>(c->meta.get(64 + (size_t)blocks * threads * 4));
+    unsigned* dout = din + 16;
+    CK(cudaMemcpyAsync(din, hin, 64, cudaMemcpyHostToDevice, c->stream));
+    for (int w = 0; w < 3; ++w) dpx_rate_kernel<<<blocks, threads, 0, c->stream>>>(din, dout, iters);
+    CK(cudaGetLastError());
+    const int reps = 10;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    for (int r = 0; r < reps; ++r) dpx_rate_kernel<<<blocks, threads, 0, c->stream>>>(din, dout, iters);
+    CK(cudaEventRecord(c->ev3, c->stream));
+    CK(cudaEventSynchronize(c->ev3));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev3));
+    *ops_per_s = (double)blocks * threads * iters * 8 * reps / (ms * 1e-3);
+  });
+}
+
+int gpusw_flush_l2(gpusw_ctx* c, int64_t bytes) {
+  return guarded(c, [&] {
+    if (bytes <= 0) return;
+    set_device(c);
+    void* p = c->flush.get((size_t)bytes);
+    CK(cudaMemsetAsync(p, 0, (size_t)bytes, c->stream));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,376 @@
+// Kernels of the scoring engine: the cross-product kernel (one column pair per CTA work
+// item, profile shared by the CTA), the pairs kernel (one pair of pairs per team, any
+// length through column passes), the per-query top-k and the residue packer.
+#pragma once
+#include "dp_core.cuh"
+
+namespace gsw {
+
+// A scored cell the int16 run could not represent; rescored by the int32 pairs kernel.
+struct Ovf {
+  int q, r;          // column (query) and row (reference) sequence
+  long long pos;     // output position
+};
+
+__device__ __forceinline__ void push_overflow(Ovf* list, int* count, int cap, int q, int r,
+                                              long long pos) {
+  int slot = atomicAdd(count, 1);
+  if (slot < cap) list[slot] = Ovf{q, r, pos};
+}
+
+// Fill the profile of one column pass: nprow rows (codes 0..ns-1 plus the pad row),
+// uint4 slot u = k4 * G + L of row a holds columns L*W + 4*k4 .. +3 (pass-relative),
+// s' = SUB[a][code] - go, or s_pad - go past a column's end / on the pad row.
+// Threads [tid0, tid0 + nthreads) of the caller cooperate.
+template <int G, int W, int P>
+__device__ __forceinline__ void build_profile(const SchemeDev& S, const int* __restrict__ sub,
+                                              const Packed& cols, int c0, int n0, int c1,
+                                              int n1, int col0, uint4* prof, int pstride,
+                                              int tid, int nthreads) {
+  constexpr int SLOTS = G * W / 4;
+  const int nprow = S.ns + 1;
+  const int pad = S.s_pad - S.go;
+  for (int idx = tid; idx < nprow * SLOTS; idx += nthreads) {
+    const int a = idx / SLOTS, u = idx - a * SLOTS;
+    const int L = u % G, k4 = u / G;
+    const int jb = col0 + L * W + 4 * k4;
+    uint32_t v[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int j = jb + e;
+      int lo = pad, hi = pad;
+      if (a < S.ns) {
+        if (c0 >= 0 && j < n0) lo = __ldg(sub + a * S.ns + cols.code(c0, j)) - S.go;
+        if (P == 2 && c1 >= 0 && j < n1) hi = __ldg(sub + a * S.ns + cols.code(c1, j)) - S.go;
+      }
+      v[e] = V<P>::pack(lo, hi);
+    }
+    prof[a * pstride + u] = make_uint4(v[0], v[1], v[2], v[3]);
+  }
+}
+
+template <int P>
+__device__ __forceinline__ Acc init_acc(const SchemeDev& S) {
+  Acc a;
+  a.best = V<P>::splat(S.mode == kModeLocal ? S.go : S.neg_low);
+  a.endrow = a.corner = a.endcol = V<P>::splat(S.neg_low);
+  return a;
+}
+
+template <int G, int P>
+__device__ __forceinline__ Acc reduce_acc(const SchemeDev& S, Acc a, unsigned wmask) {
+  a.best = team_max<G, P>(a.best, wmask);
+  if (S.mode != kModeLocal) {
+    a.endrow = team_max<G, P>(a.endrow, wmask);
+    a.corner = team_max<G, P>(a.corner, wmask);
+    a.endcol = team_max<G, P>(a.endcol, wmask);
+  }
+  return a;
+}
+
+// -------------------------------------------------------------------------------------
+// Cross product: work item = (column pair, chunk of `rows_per_item` rows). The CTA builds
+// the pair's profile once and its teams walk the chunk's rows.
+struct CrossParams {
+  SchemeDev S;
+  const int* sub;
+  Packed cols, rows;
+  const int2* pairs;       // column sequences of each pair (c1 = -1: none)
+  const int2* pair_out;    // output row of each half in `out`
+  const int* row_perm;     // row sequences, longest first
+  int n_rows, rows_per_item;
+  const int2* items;       // (pair, chunk), costliest first
+  int n_items;
+  int* queue;              // work counter, zero at launch
+  int* out;                // int32 scores, out[out_row * out_ld + row_seq]
+  long long out_ld;
+  Ovf* ovf;
+  int* ovf_count;
+  int ovf_cap;
+};
+
+template <int G, int W, int P, bool LOCAL>
+__global__ void __launch_bounds__(256) cross_kernel(const CrossParams p) {
+  extern __shared__ uint4 smem_prof[];
+  __shared__ int s_item;
+  constexpr int SLOTS = G * W / 4;
+  const int pstride = (SLOTS + 7) & ~7;
+  const int team = threadIdx.x / G, lane = threadIdx.x % G, nteams = blockDim.x / G;
+  const unsigned wmask = (G == 32) ? 0xFFFFFFFFu
+                                   : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(p.queue, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();
+    if (it >= p.n_items) break;
+    const int2 item = p.items[it];
+    const int2 pr = p.pairs[item.x], po = p.pair_out[item.x];
+    const int n0 = pr.x >= 0 ? p.cols.len[pr.x] : 0;
+    const int n1 = (P == 2 && pr.y >= 0) ? p.cols.len[pr.y] : 0;
+    build_profile<G, W, P>(p.S, p.sub, p.cols, pr.x, n0, P == 2 ? pr.y : -1, n1, 0, smem_prof,
+                           pstride, threadIdx.x, blockDim.x);
+    __syncthreads();
+    const int r_begin = item.y * p.rows_per_item;
+    const int r_end = min(p.n_rows, r_begin + p.rows_per_item);
+    for (int rr = r_begin + team; rr < r_end; rr += nteams) {
+      const int rs = p.row_perm[rr];
+      const int m = p.rows.len[rs];
+      Acc acc = init_acc<P>(p.S);
+      if (m > 0 && max(n0, n1) > 0) {
+        team_pass<G, W, P, LOCAL, false>(p.S, smem_prof, pstride, p.rows.words + p.rows.woff[rs],
+                                         nullptr, p.rows.bits, p.rows.per, m, m, n0, n1, 0,
+                                         nullptr, false, false, lane, wmask, acc);
+        acc = reduce_acc<G, P>(p.S, acc, wmask);
+      }
+      if (lane == 0) {
+#pragma unroll
+        for (int h = 0; h < P; ++h) {
+          const int c = h ? pr.y : pr.x;
+          if (c < 0) continue;
+          const int nh = h ? n1 : n0;
+          const long long pos = (long long)(h ? po.y : po.x) * p.out_ld + rs;
+          bool ovf = false;
+          int score = (m == 0 || nh == 0) ? empty_score(p.S, nh, m)
+                                           : finish_score<P>(p.S, acc, h, &ovf);
+          if (P == 2 && ovf && m > 0 && nh > 0) {
+            push_overflow(p.ovf, p.ovf_count, p.ovf_cap, c, rs, pos);
+            score = INT_MIN;
+          }
+          p.out[pos] = score;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// Pairs: work item = P alignments (one per register half), each with its own column and
+// row sequence. The team builds its own profile for every column pass; passes hand the
+// boundary column over through a per-team scratch strip in global memory.
+struct PairsParams {
+  SchemeDev S;
+  const int* sub;
+  Packed cols, rows;
+  // Item sources (exactly one is used):
+  //  explicit: alignment a of item t is order[t * P + a] -> (qi, rj, pos = index)
+  //  overflow: alignment t is ovf[t] (P == 1), n_items = min(*ovf_count, ovf_cap)
+  //  cross:    item t = (pair t / n_rows, row_perm[t % n_rows]) with pairs/pair_out
+  const int* qi;
+  const int* rj;
+  const int* order;
+  long long n_align;         // explicit mode: number of alignments
+  const Ovf* ovf_in;
+  const int* ovf_in_count;
+  int ovf_in_cap;
+  const int2* pairs;
+  const int2* pair_out;
+  const int* row_perm;
+  int n_rows;
+  long long out_ld;
+  long long n_items;         // explicit / cross
+  int item_mode;             // 0 explicit, 1 overflow, 2 cross
+  unsigned long long* queue; // work counter, zero at launch
+  int* out;
+  uint2* bnd;                // per-team boundary strips
+  int bnd_cap;               // rows per strip
+  Ovf* ovf;                  // int16 overflow output
+  int* ovf_count;
+  int ovf_cap;
+};
+
+template <int P>
+struct PairItem {
+  int q[P], r[P];
+  long long pos[P];
+  bool valid[P];
+};
+
+template <int P>
+__device__ __forceinline__ PairItem<P> decode_item(const PairsParams& p, long long t) {
+  PairItem<P> it;
+#pragma unroll
+  for (int a = 0; a < P; ++a) {
+    it.valid[a] = false;
+    it.q[a] = it.r[a] = -1;
+    it.pos[a] = -1;
+    if (p.item_mode == 0) {
+      const long long k = t * P + a;
+      if (k < p.n_align) {
+        const int idx = p.order ? p.order[k] : (int)k;
+        it.q[a] = p.qi[idx];
+        it.r[a] = p.rj[idx];
+        it.pos[a] = idx;
+        it.valid[a] = true;
+      }
+    } else if (p.item_mode == 1) {
+      const Ovf o = p.ovf_in[t];
+      it.q[a] = o.q;
+      it.r[a] = o.r;
+      it.pos[a] = o.pos;
+      it.valid[a] = true;
+    } else {
+      const int pi = (int)(t / p.n_rows);
+      const int rs = p.row_perm[t % p.n_rows];
+      const int2 pr = p.pairs[pi], po = p.pair_out[pi];
+      const int c = a ? pr.y : pr.x;
+      if (c >= 0) {
+        it.q[a] = c;
+        it.r[a] = rs;
+        it.pos[a] = (long long)(a ? po.y : po.x) * p.out_ld + rs;
+        it.valid[a] = true;
+      }
+    }
+  }
+  return it;
+}
+
+template <int G, int W, int P, bool LOCAL>
+__global__ void __launch_bounds__(256) pairs_kernel(const PairsParams p) {
+  extern __shared__ uint4 smem_prof[];
+  constexpr int SLOTS = G * W / 4;
+  const int pstride = (SLOTS + 7) & ~7;
+  const int team = threadIdx.x / G, lane = threadIdx.x % G, nteams = blockDim.x / G;
+  const unsigned wmask = (G == 32) ? 0xFFFFFFFFu
+                                   : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
+  uint4* prof = smem_prof + (size_t)team * (p.S.ns + 1) * pstride;
+  uint2* bnd = p.bnd ? p.bnd + ((size_t)blockIdx.x * nteams + team) * p.bnd_cap : nullptr;
+  long long n_items = p.n_items;
+  if (p.item_mode == 1) n_items = min(*p.ovf_in_count, p.ovf_in_cap);
+  for (;;) {
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(p.queue, 1ull);
+    t = __shfl_sync(wmask, t, 0, G);
+    if ((long long)t >= n_items) break;
+    const PairItem<P> it = decode_item<P>(p, (long long)t);
+    int n[P], m[P];
+#pragma unroll
+    for (int a = 0; a < P; ++a) {
+      n[a] = it.valid[a] ? p.cols.len[it.q[a]] : 0;
+      m[a] = it.valid[a] ? p.rows.len[it.r[a]] : 0;
+    }
+    const int n0 = n[0], m0 = m[0];
+    const int n1 = P == 2 ? n[1] : 0, m1 = P == 2 ? m[1] : 0;
+    const int ncols = max(n0, n1), mrows = max(m0, m1);
+    Acc acc = init_acc<P>(p.S);
+    if (ncols > 0 && mrows > 0) {
+      const int npass = (ncols + G * W - 1) / (G * W);
+      const uint32_t* w0 = p.rows.words + p.rows.woff[max(it.r[0], 0)];
+      const uint32_t* w1 = (P == 2 && it.r[P - 1] >= 0) ? p.rows.words + p.rows.woff[it.r[P - 1]] : w0;
+      for (int ps = 0; ps < npass; ++ps) {
+        __syncwarp(wmask);
+        build_profile<G, W, P>(p.S, p.sub, p.cols, it.valid[0] ? it.q[0] : -1, n0,
+                               (P == 2 && it.valid[P - 1]) ? it.q[P - 1] : -1, n1, ps * G * W,
+                               prof, pstride, lane, G);
+        __syncwarp(wmask);
+        team_pass<G, W, P, LOCAL, true>(p.S, prof, pstride, w0, w1, p.rows.bits, p.rows.per,
+                                        m0, P == 2 ? m1 : m0, n0, n1, ps * G * W, bnd, ps > 0,
+                                        ps + 1 < npass, lane, wmask, acc);
+      }
+      acc = reduce_acc<G, P>(p.S, acc, wmask);
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int a = 0; a < P; ++a) {
+        if (!it.valid[a]) continue;
+        bool ovf = false;
+        int score = (n[a] == 0 || m[a] == 0) ? empty_score(p.S, n[a], m[a])
+                                             : finish_score<P>(p.S, acc, a, &ovf);
+        if (P == 2 && ovf && n[a] > 0 && m[a] > 0) {
+          push_overflow(p.ovf, p.ovf_count, p.ovf_cap, it.q[a], it.r[a], it.pos[a]);
+          score = INT_MIN;
+        }
+        p.out[it.pos[a]] = score;
+      }
+    }
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// Per-row top-k of an int32 score matrix in the order (score descending, index ascending):
+// key = (score with its sign bit flipped) << 32 | ~index, so a larger key ranks first and
+// no two keys tie. Each round keeps, per thread, the best 32 keys below the previous
+// round's last key, then merges them warp by warp; ceil(k / 32) rounds.
+constexpr int kTopkPer = 32;
+
+__device__ __forceinline__ unsigned long long topk_key(int score, int idx) {
+  return ((unsigned long long)((unsigned)score ^ 0x80000000u) << 32) | (unsigned)(~idx);
+}
+
+__global__ void __launch_bounds__(256) topk_kernel(const int* __restrict__ scores, long long ld,
+                                                   int ncols, int k, int* out_idx,
+                                                   int* out_score, long long out_ld) {
+  __shared__ unsigned long long s_keys[8][kTopkPer];
+  __shared__ unsigned long long s_last;
+  const int row = blockIdx.x;
+  const int* srow = scores + (long long)row * ld;
+  const int warp = threadIdx.x / 32, ln = threadIdx.x % 32, nw = blockDim.x / 32;
+  const int kk = min(k, ncols);
+  unsigned long long bound = ~0ull;  // keys must be strictly below this
+  int done = 0;
+  while (done < kk) {
+    const int want = min(kTopkPer, kk - done);
+    unsigned long long lst[kTopkPer];
+#pragma unroll
+    for (int s = 0; s < kTopkPer; ++s) lst[s] = 0ull;
+    for (int j = threadIdx.x; j < ncols; j += blockDim.x) {
+      const unsigned long long key = topk_key(srow[j], j);
+      if (key >= bound || key <= lst[kTopkPer - 1]) continue;
+      // insert into the descending list
+      unsigned long long cur = key;
+#pragma unroll
+      for (int s = 0; s < kTopkPer; ++s) {
+        const unsigned long long hi = cur > lst[s] ? cur : lst[s];
+        cur = cur > lst[s] ? lst[s] : cur;
+        lst[s] = hi;
+      }
+    }
+    // warp merge: `want` rounds of arg-max over the lanes' list heads
+    int head = 0;
+    for (int s = 0; s < want; ++s) {
+      unsigned long long mine = head < kTopkPer ? lst[0] : 0ull;
+      unsigned long long best = mine;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        unsigned long long o = __shfl_xor_sync(0xFFFFFFFFu, best, off);
+        best = o > best ? o : best;
+      }
+      if (ln == 0) s_keys[warp][s] = best;
+      if (best != 0ull && mine == best) {  // pop my head
+#pragma unroll
+        for (int q = 0; q + 1 < kTopkPer; ++q) lst[q] = lst[q + 1];
+        lst[kTopkPer - 1] = 0ull;
+        ++head;
+      }
+    }
+    __syncthreads();
+    // block merge by warp 0 over the nw sorted lists
+    if (warp == 0) {
+      int pos = 0;  // my list is s_keys[ln] for ln < nw
+      for (int s = 0; s < want; ++s) {
+        unsigned long long mine = (ln < nw && pos < want) ? s_keys[ln][pos] : 0ull;
+        unsigned long long best = mine;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          unsigned long long o = __shfl_xor_sync(0xFFFFFFFFu, best, off);
+          best = o > best ? o : best;
+        }
+        if (best != 0ull && mine == best) ++pos;
+        if (ln == 0) {
+          const int idx = (int)(~(unsigned)(best & 0xFFFFFFFFull));
+          const int sc = (int)((unsigned)(best >> 32) ^ 0x80000000u);
+          out_idx[(long long)row * out_ld + done + s] = idx;
+          out_score[(long long)row * out_ld + done + s] = sc;
+          if (s == want - 1) s_last = best;
+        }
+      }
+    }
+    __syncthreads();
+    bound = s_last;
+    done += want;
+    __syncthreads();
+  }
+}
+
+}  // namespace gsw

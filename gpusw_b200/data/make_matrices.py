@@ -1,0 +1,48 @@
+"""Regenerate the bundled substitution tables from the reference package's data files.
+
+The scores must be identical to the reference's (``src/gpusw/data/matrices/*.txt``,
+public NCBI/Biopython tables), so this script parses each of the reference's files and
+writes the same alphabet and integers back out in NCBI text format with a short header of
+our own. It only runs in a checkout that has the reference next to it:
+
+    python gpusw_b200/data/make_matrices.py /root/reference/src/gpusw/data/matrices
+"""
+from __future__ import annotations
+
+import pathlib
+import sys
+
+HERE = pathlib.Path(__file__).resolve().parent / "matrices"
+
+
+def _read(path: pathlib.Path) -> tuple[list[str], list[list[int]]]:
+    header = None
+    rows = []
+    for line in path.read_text().splitlines():
+        s = line.strip()
+        if not s or s.startswith("#") or s.startswith("//"):
+            continue
+        f = s.split()
+        if header is None:
+            header = f
+            continue
+        rows.append([int(round(float(v))) for v in f[1:]])
+    return header, rows
+
+
+def main(src_dir: str) -> None:
+    src = pathlib.Path(src_dir)
+    for path in sorted(src.glob("*.txt")):
+        syms, rows = _read(path)
+        width = max(len(str(v)) for r in rows for v in r) + 2
+        lines = [f"# {path.stem}: integer substitution scores, rows = reference residue,",
+                 "# columns = query residue (NCBI text format)"]
+        lines.append(" " + "".join(s.rjust(width) for s in syms))
+        for sym, row in zip(syms, rows, strict=True):
+            lines.append(sym + "".join(str(v).rjust(width) for v in row))
+        (HERE / path.name).write_text("\n".join(lines) + "\n")
+        print("wrote", HERE / path.name)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/gpusw/data/matrices")

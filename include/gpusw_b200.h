@@ -1,0 +1,150 @@
+/*
+ * gpusw_b200.h -- C ABI of the B200 Gotoh scoring engine (libgpusw_sm100.so).
+ *
+ * Plain C types only: pointers, sizes and int status codes. No exception crosses the ABI;
+ * every call returns GPUSW_OK (0) or an error code, and gpusw_last_error() gives the
+ * message. A context owns one CUDA stream on one device plus every device buffer it
+ * allocates; calls on one context must be serialised by the caller (one context per host
+ * thread, or a lock around it). Host buffers passed in or out belong to the caller.
+ *
+ * Each entry point names the interface of the reference package (freiburgermsu/gpuSW,
+ * Python) that it replaces; see INTEGRATION.md for the ctypes binding.
+ */
+#ifndef GPUSW_B200_H
+#define GPUSW_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The Python layer maps them onto the reference's exception classes
+ * (src/gpusw/errors.py:5-31): INVALID -> ValueError, NO_GPU -> NoGpuError,
+ * SCHEME -> SchemeError, OVERFLOW -> OverflowRiskError, the rest -> GpuSWError. */
+#define GPUSW_OK 0
+#define GPUSW_ERR_INVALID 1      /* bad argument: null pointer, index out of range, ... */
+#define GPUSW_ERR_NO_GPU 2       /* no CUDA device / driver */
+#define GPUSW_ERR_CUDA 3         /* a CUDA call failed */
+#define GPUSW_ERR_MEMORY 4       /* device memory budget exceeded / allocation failed */
+#define GPUSW_ERR_OVERFLOW 5     /* scores cannot be represented even in int32 */
+#define GPUSW_ERR_SCHEME 6       /* no scheme set, or scheme values out of range */
+#define GPUSW_ERR_QUEUE_FULL 7   /* serving: admission refused (no slot / memory) */
+#define GPUSW_ERR_NOT_FOUND 8    /* unknown handle or request id */
+#define GPUSW_ERR_CANCELLED 9    /* serving: the request was cancelled */
+#define GPUSW_ERR_TIMEOUT 10     /* a bounded wait ran out */
+
+/* Alignment modes (src/gpusw/scheme.py:19, MODES). */
+#define GPUSW_MODE_LOCAL 0
+#define GPUSW_MODE_GLOBAL 1
+#define GPUSW_MODE_SEMIGLOBAL 2
+
+/* Integer width policy (src/gpusw/scheme.py:116-141, Scheme.resolve_dtype).
+ * AUTO: every pair in int16 (two alignments per 32-bit register); pairs whose int16 run
+ * may have overflowed are rescored in int32 -- the integers equal an all-int32 run.
+ * INT16: same kernels; the caller has already checked the static envelope.
+ * INT32: every pair in int32. */
+#define GPUSW_DTYPE_AUTO 0
+#define GPUSW_DTYPE_INT16 1
+#define GPUSW_DTYPE_INT32 2
+
+typedef struct gpusw_ctx gpusw_ctx;
+
+/* Counters of the last call and of the context's lifetime. Times come from CUDA events
+ * recorded on the context's stream. */
+typedef struct gpusw_stats {
+  double last_kernel_ms;      /* scoring + rescoring + top-k kernels of the last call */
+  double last_total_ms;       /* the last call's device work including its copies */
+  double last_cells;          /* DP cells of the last call (sum of |q| * |r|) */
+  int64_t last_pairs;         /* alignments scored by the last call */
+  int64_t last_overflow;      /* int16 cells rescored in int32 by the last call */
+  int64_t last_launches;      /* kernels launched by the last call */
+  int64_t total_launches;     /* kernels launched by this context */
+  int64_t total_overflow;     /* int16 rescores over the context's lifetime */
+  int64_t device_bytes;       /* device memory currently held by the context */
+} gpusw_stats;
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int gpusw_version(void);
+
+/* Number of visible CUDA devices (0 when there is no driver/GPU; never an error).
+ * Replaces src/gpusw/_compile.py:39-46 (gpu_available). */
+int gpusw_device_count(int *count);
+
+/* Create / destroy a context on `device`. Replaces the device binding of
+ * src/gpusw/backends/cuda.py:30-35 (device_scope). */
+int gpusw_ctx_create(int device, gpusw_ctx **out);
+void gpusw_ctx_destroy(gpusw_ctx *ctx);
+
+/* Message of the last failed call on `ctx` (or of the last failed gpusw_ctx_create when
+ * ctx is NULL). Valid until the next call on the context. */
+const char *gpusw_last_error(const gpusw_ctx *ctx);
+
+/* Set the scoring scheme: mode, gap open/extend (<= 0), semiglobal free-end flags, and the
+ * (ns x ns) int32 substitution table, row = reference code, column = query code, last
+ * row/column = sentinel. Replaces src/gpusw/_compile.py:55-93 (get_module: the baked
+ * MODE/GOPEN/GEXT/FREE_Q/FREE_R/NS, and get_sub: the SUB upload). */
+int gpusw_set_scheme(gpusw_ctx *ctx, int mode, int gap_open, int gap_extend, int free_q,
+                     int free_r, int ns, const int32_t *sub);
+
+/* Upload one encoded sequence set (codes in [0, ns), offsets[n + 1], int32 like the
+ * reference's Encoded). The library packs it (2, 4, 5 or 8 bits per residue, picked from
+ * the largest code) and keeps it resident; *out_db receives the handle. Replaces
+ * src/gpusw/backends/__init__.py:57-59 (Backend.upload of codes and offsets). */
+int gpusw_db_upload(gpusw_ctx *ctx, const uint8_t *codes, const int32_t *offsets, int32_t n,
+                    int32_t *out_db);
+
+/* Release a sequence set. */
+int gpusw_db_free(gpusw_ctx *ctx, int32_t db);
+
+/* Bits per residue the set was packed with, or a negative status. */
+int gpusw_db_bits(gpusw_ctx *ctx, int32_t db);
+
+/* Cross product: out[a * n_refs + b] = score(query qlist[a] of qdb, reference b of rdb),
+ * int32, host buffer of nq * n_refs. Replaces src/gpusw/backends/cuda.py:47-66 (run_cross)
+ * and :87-91 (as_host), kernel sw_cross of src/gpusw/kernel.py:161-175. */
+int gpusw_score_cross(gpusw_ctx *ctx, int32_t qdb, int32_t rdb, const int32_t *qlist,
+                      int32_t nq, int dtype, int32_t *out);
+
+/* Per-query top-k: out_idx/out_score are host (nq, min(k, n_refs)) int32, best first,
+ * ties broken by the lower reference index (the order of a stable sort of -scores).
+ * Queries are scored in blocks that keep the score block within the context's memory
+ * budget. Replaces src/gpusw/aligner.py:169-195 (Aligner.top_k) together with
+ * src/gpusw/backends/cuda.py:93-106 (Backend.topk). */
+int gpusw_topk(gpusw_ctx *ctx, int32_t qdb, int32_t rdb, const int32_t *qlist, int32_t nq,
+               int32_t k, int dtype, int32_t *out_idx, int32_t *out_score);
+
+/* Explicit pairs: out[i] = score(query qi[i] of qdb, reference rj[i] of rdb). Indices are
+ * validated before any launch (GPUSW_ERR_INVALID on an out-of-range index). Replaces
+ * src/gpusw/backends/cuda.py:68-85 (run_pairs), kernel sw_pairs of
+ * src/gpusw/kernel.py:178-190. */
+int gpusw_score_pairs(gpusw_ctx *ctx, int32_t qdb, int32_t rdb, const int32_t *qi,
+                      const int32_t *rj, int64_t n, int dtype, int32_t *out);
+
+/* Engine options. plain != 0 selects the one-batch-per-call form (queries in input order,
+ * one kernel shape per batch, no length binning, no graph) used as the comparison point
+ * of the batched form. mem_budget bounds the score blocks of gpusw_topk (bytes, 0 keeps the
+ * default of 4 GiB). */
+int gpusw_set_options(gpusw_ctx *ctx, int plain, int64_t mem_budget);
+
+/* Counters (see gpusw_stats). Replaces src/gpusw/aligner.py:212 (Aligner.gcups): GCUPS =
+ * last_cells / last_kernel_ms / 1e6. */
+int gpusw_get_stats(gpusw_ctx *ctx, gpusw_stats *out);
+
+/* Block until the context's stream is idle. */
+int gpusw_sync(gpusw_ctx *ctx);
+
+/* Sustained int16x2 add-max (DPX) instruction rate of the device, measured by a short
+ * self-timed kernel: *ops_per_s lane-operations per second. The denominator of the
+ * scoring kernels' instruction roofline. No reference counterpart (measurement only). */
+int gpusw_measure_dpx_rate(gpusw_ctx *ctx, double *ops_per_s);
+
+/* Write `bytes` of zeros into a scratch buffer on the context's stream (evicts the L2
+ * between timed steps of a benchmark). No reference counterpart (measurement only). */
+int gpusw_flush_l2(gpusw_ctx *ctx, int64_t bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPUSW_B200_H */

@@ -1,0 +1,410 @@
+#!/usr/bin/env python
+"""Benchmark of the Gotoh scoring engine on B200: GCUPS (giga DP-cell updates per second).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload 16s|protein|pairs|small]
+                    [--impl ours|reference]
+
+Default workload: the 16S-shaped exhaustive search -- 2,000 queries (250-253 nt) against
+20,000 references (~1,400-1,600 nt) made from 300 mutated ancestors, DNA local
+2/-3/-5/-2, int16 with int32 rescoring, per-query top-5 (synthetic, seeded). One step
+scores the whole cross product (1.5e13 cells) and selects the top-5 of every query.
+
+* ``value``: batched form, inputs resident in HBM, device time of the step from CUDA events
+  on the engine's stream, L2 flushed (256 MiB memset) before every timed step; summed over
+  K steps and maxed over ranks.
+* ``e2e``: the same step through the C ABI with host buffers: upload of the encoded query
+  and reference sets (host -> device), scoring, top-k, copy of the top-k back; wall time.
+* ``plain``: the same kernels in the one-batch-per-call form (16 queries per call, input
+  order, one kernel shape per call, no length binning), for the batched/plain ratio.
+* ``roofline``: the scoring kernels against the int16x2 instruction roofline -- the DPX
+  add-max rate measured live on this GPU x 2 cells / 5.5 instructions per cell pair.
+* ``cpu_baseline`` / ``--impl reference``: the C restatement of the reference's oracle on
+  all host cores, on a bounded seeded sample of the same workload.
+
+With torchrun and N > 1 every rank runs an independent replica of the workload on its own
+GPU (the scoring path has no exchange step); ``value`` = N x cells / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GCUPS on 1 B200 (bit-exact) batched/served vs plain; p50/p99 request latency"
+OPS_PER_CELL_PAIR = 5.5  # int16x2 instructions per register of two cells (see dp_core.cuh)
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="16s", choices=["16s", "protein", "pairs", "small"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--plain-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+class Group:
+    """Host-side barrier and max-reduction across replicas (gloo; no data-path exchange)."""
+
+    def __init__(self, world: int):
+        self.world = world
+        self.dist = None
+        if world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.dist:
+            return x
+        import torch
+
+        t = torch.tensor([float(x)], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.destroy_process_group()
+
+
+def workload(name: str):
+    from gpusw_b200 import workloads
+
+    return workloads.by_name(name)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as fh:
+            for line in fh:
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].replace(".", "").isdigit():
+                    rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]),
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+# ------------------------------------------------------------------------------ CPU side
+def cpu_sample(wl, seconds: float, rng_seed: int = 99):
+    """A seeded subsample of the workload sized to about `seconds` of oracle time on all
+    host threads; returns (q_enc, r_enc, q_idx, r_idx, cells, gcups, threads)."""
+    import oracle
+    from gpusw_b200.encode import Encoded
+
+    def enc(codes, offs):
+        return Encoded(codes, offs, list(range(offs.shape[0] - 1)), np.diff(offs).astype(np.int32),
+                       wl.scheme.eff_alphabet)
+
+    q = enc(*wl.queries)
+    r = enc(*wl.refs)
+    threads = os.cpu_count() or 1
+    rng = np.random.default_rng(rng_seed)
+    if wl.pairs is not None:
+        def run(n):
+            sel = rng.choice(wl.pairs[0].shape[0], size=n, replace=False).astype(np.int32)
+            qi, rj = wl.pairs[0][sel], wl.pairs[1][sel]
+            t0 = time.perf_counter()
+            oracle.score_pairs(q, r, qi, rj, wl.scheme, threads=threads)
+            dt = time.perf_counter() - t0
+            cells = float((q.lengths[qi].astype(np.float64) * r.lengths[rj]).sum())
+            return (qi, rj), cells, dt
+        sample, cells, dt = run(2000)
+        rate = cells / dt
+        n = int(min(wl.pairs[0].shape[0], max(2000, 2000 * seconds * rate / cells)))
+        sample, cells, dt = run(n)
+    else:
+        def run(nq, nr):
+            qi = np.sort(rng.choice(q.n, size=min(nq, q.n), replace=False)).astype(np.int32)
+            rj = np.sort(rng.choice(r.n, size=min(nr, r.n), replace=False)).astype(np.int32)
+            rsub = enc(*subset(wl.refs, rj))
+            t0 = time.perf_counter()
+            oracle.score_cross(q, rsub, wl.scheme, qlist=qi, threads=threads)
+            dt = time.perf_counter() - t0
+            cells = float(q.lengths[qi].astype(np.float64).sum() * rsub.lengths.astype(np.float64).sum())
+            return (qi, rj), cells, dt
+        nq0 = min(q.n, 16)
+        sample, cells, dt = run(nq0, min(r.n, 64))
+        rate = cells / dt
+        target = seconds * rate
+        nr = int(min(r.n, max(64, target / max(1.0, q.lengths.mean() * nq0 * r.lengths.mean()))))
+        sample, cells, dt = run(nq0, nr)
+    return sample, cells, cells / dt / 1e9, threads, dt
+
+
+def subset(enc_pair, idx):
+    codes, offs = enc_pair
+    lens = np.diff(offs)[idx]
+    new_offs = np.zeros(idx.shape[0] + 1, dtype=np.int64)
+    np.cumsum(lens, out=new_offs[1:])
+    parts = [codes[offs[i]:offs[i + 1]] for i in idx]
+    return (np.concatenate(parts) if parts else np.zeros(0, np.uint8), new_offs.astype(np.int32))
+
+
+def config_of(wl) -> dict:
+    cfg = {"workload": {"16s": "16S-shaped exhaustive search, top-5",
+                        "protein": "uneven-length protein batch, top-10",
+                        "pairs": "paired semiglobal read scoring",
+                        "small": "small DNA cross product, int32"}[wl.name],
+           "queries": wl.nq, "refs": wl.nr, "cells": wl.cells(), "k": wl.k or None,
+           "scheme": f"{wl.scheme.mode} {'matrix ' + wl.scheme.matrix.name if wl.scheme.matrix is not None else f'{wl.scheme.match}/{wl.scheme.mismatch}'} "
+                     f"gaps {wl.scheme.gap_open}/{wl.scheme.gap_extend}",
+           "dtype_policy": wl.scheme.dtype, "seed": wl.seed, "synthetic": wl.note,
+           "l2": "flushed (256 MiB memset) before every timed step",
+           "parallelism": "replicas"}
+    return cfg
+
+
+def run_reference(args, rank):
+    """The reference arm: the oracle restatement of the reference's CPU scorer on all host
+    threads, each step a bounded seeded sample of the workload."""
+    if rank != 0:
+        return
+    wl = workload(args.workload)
+    per_step = []
+    threads = os.cpu_count() or 1
+    sample_desc = ""
+    for s in range(args.warmup + args.steps):
+        sample, cells, gcups, threads, dt = cpu_sample(wl, min(args.cpu_seconds, 10.0), rng_seed=1000 + s)
+        if s >= args.warmup:
+            per_step.append((cells, dt))
+        sample_desc = (f"{len(sample[0])} x {len(sample[1])} seeded subsample per step" if wl.pairs is None
+                       else f"{len(sample[0])} seeded pairs per step")
+    cells = sum(c for c, _ in per_step)
+    secs = sum(t for _, t in per_step)
+    v = cells / secs / 1e9
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GCUPS", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / len(per_step) * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+           "data": "synthetic", "config": config_of(wl),
+           "cpu_baseline": {"value": v, "unit": "GCUPS", "cores": threads, "kind": "port",
+                            "sample": sample_desc},
+           "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def packed_bytes(offs: np.ndarray, bits: int) -> int:
+    per = 6 if bits == 5 else 32 // bits
+    lens = np.diff(offs).astype(np.int64)
+    words = ((lens + per - 1) // per + 3) // 4 * 4
+    return int(words.sum() * 4 + 64 * 4 + lens.shape[0] * 20)
+
+
+def run_ours(args, rank, world, local):
+    from gpusw_b200 import _native
+
+    group = Group(world)
+    wl = workload(args.workload)
+    ctx = _native.context(local)
+    ctx.set_scheme(wl.scheme)
+    qdb = ctx.upload(*wl.queries)
+    rdb = ctx.upload(*wl.refs)
+    policy = wl.scheme.dtype
+    qlist = np.arange(wl.nq, dtype=np.int32)
+    cells = wl.cells()
+
+    def step():
+        if wl.pairs is not None:
+            ctx.score_pairs(qdb, rdb, wl.pairs[0], wl.pairs[1], policy)
+        else:
+            ctx.topk(qdb, rdb, qlist, wl.nr, wl.k, policy)
+        return ctx.stats()
+
+    dpx = ctx.dpx_rate()
+    for _ in range(args.warmup):
+        step()
+    sampler = ClockSampler(local)
+    ctx.sync()
+    group.barrier()
+    sampler.start()
+    times, score_ms, topk_ms, launches, ovf = [], [], [], 0, 0
+    for _ in range(args.steps):
+        ctx.flush_l2(L2_FLUSH_BYTES)
+        st = step()
+        times.append(st.last_total_ms)
+        score_ms.append(st.last_score_ms)
+        topk_ms.append(st.last_topk_ms)
+        launches += st.last_launches
+        ovf += st.last_overflow
+    ctx.sync()
+    group.barrier()
+    clocks = sampler.stop()
+    total_ms = group.max(sum(times))
+    value = world * cells * args.steps / (total_ms * 1e-3) / 1e9
+    kern_gcups = cells * args.steps / (sum(score_ms) * 1e-3) / 1e9
+    peak_gcups = dpx * 2.0 / OPS_PER_CELL_PAIR / 1e9
+
+    # plain (one batch per call) form of the same kernels
+    plain = None
+    if args.plain_steps > 0:
+        ctx.set_options(plain=True)
+        step()
+        pt = []
+        for _ in range(args.plain_steps):
+            ctx.flush_l2(L2_FLUSH_BYTES)
+            t0 = time.perf_counter()
+            if wl.pairs is not None:
+                ctx.score_pairs(qdb, rdb, wl.pairs[0], wl.pairs[1], policy)
+            else:
+                ctx.topk(qdb, rdb, qlist, wl.nr, wl.k, policy)
+            pt.append(time.perf_counter() - t0)
+        ctx.set_options(plain=False)
+        p_s = group.max(sum(pt))
+        plain = {"value": world * cells * args.plain_steps / p_s / 1e9, "unit": "GCUPS",
+                 "form": "16 queries per call, input order, one kernel shape per call, wall time"}
+
+    # end to end through the C ABI with host buffers
+    e2e_t = []
+    h2d = d2h = 0
+    for _ in range(args.e2e_steps):
+        ctx.sync()
+        t0 = time.perf_counter()
+        q2 = ctx.upload(*wl.queries)
+        r2 = ctx.upload(*wl.refs)
+        if wl.pairs is not None:
+            ctx.score_pairs(q2, r2, wl.pairs[0], wl.pairs[1], policy)
+            d2h = wl.pairs[0].shape[0] * 4
+            h2d_extra = wl.pairs[0].nbytes * 3
+        else:
+            idx, sc = ctx.topk(q2, r2, qlist, wl.nr, wl.k, policy)
+            d2h = idx.nbytes + sc.nbytes
+            h2d_extra = qlist.nbytes
+        e2e_t.append(time.perf_counter() - t0)
+        h2d = packed_bytes(wl.queries[1], ctx.bits(q2)) + packed_bytes(wl.refs[1], ctx.bits(r2)) + h2d_extra
+        ctx.free(q2)
+        ctx.free(r2)
+    e2e = None
+    if e2e_t:
+        e_s = group.max(sum(e2e_t))
+        e2e = {"value": world * cells * len(e2e_t) / e_s / 1e9, "unit": "GCUPS",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "timing": "wall clock around upload + score + top-k + copy back"}
+
+    # CPU oracle baseline and a bit-exact check of the same sample (rank 0, N = 1)
+    cpu = None
+    bitexact = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        import oracle
+        from gpusw_b200.encode import Encoded
+
+        sample, c_cells, c_gcups, threads, c_dt = cpu_sample(wl, args.cpu_seconds)
+        cpu = {"value": c_gcups, "unit": "GCUPS", "cores": threads, "kind": "port",
+               "sample": (f"{len(sample[0])} queries x {len(sample[1])} refs of the workload, "
+                          f"{c_cells:.3e} cells, {c_dt:.1f} s" if wl.pairs is None else
+                          f"{len(sample[0])} pairs of the workload, {c_cells:.3e} cells, {c_dt:.1f} s")}
+        # bit-exactness of the GPU on that sample
+        def as_enc(codes, offs):
+            return Encoded(codes, offs, list(range(offs.shape[0] - 1)),
+                           np.diff(offs).astype(np.int32), wl.scheme.eff_alphabet)
+
+        q = as_enc(*wl.queries)
+        if wl.pairs is None:
+            rsub = subset(wl.refs, sample[1])
+            r = as_enc(*rsub)
+            want = oracle.score_cross(q, r, wl.scheme, qlist=sample[0])
+            rd = ctx.upload(*rsub)
+            got = ctx.score_cross(qdb, rd, sample[0], len(sample[1]), policy)
+            ctx.free(rd)
+        else:
+            r = as_enc(*wl.refs)
+            want = oracle.score_pairs(q, r, sample[0], sample[1], wl.scheme)
+            got = ctx.score_pairs(qdb, rdb, sample[0], sample[1], policy)
+        bitexact = {"pairs_checked": int(np.asarray(want).size),
+                    "equal": bool(np.array_equal(np.asarray(got, dtype=np.int64), want))}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup,
+               "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "int16x2 (int32 rescoring)" if policy != "int32" else "int32",
+               "data": "synthetic", "config": config_of(wl), "gpu_launches": launches,
+               "roofline": {"bound": "int", "achieved": kern_gcups, "peak": peak_gcups,
+                            "unit": "GCUPS", "frac": kern_gcups / peak_gcups,
+                            "traffic": None,
+                            "peak_source": f"measured s16x2 add-max rate {dpx / 1e12:.2f} Tops/s x 2 cells"
+                                           f" / {OPS_PER_CELL_PAIR} ops (live, this GPU)",
+                            "kernel_ms_per_step": sum(score_ms) / args.steps,
+                            "topk_ms_per_step": sum(topk_ms) / args.steps},
+               "plain": plain, "batched_over_plain": (value / plain["value"]) if plain else None,
+               "e2e": e2e, "cpu_baseline": cpu, "bitexact_sample": bitexact,
+               "overflow_rescored": ovf, "clocks": clocks}
+        print(json.dumps(out), flush=True)
+    group.close()
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

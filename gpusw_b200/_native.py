@@ -31,6 +31,8 @@ _lib_lock = threading.Lock()
 class Stats(ctypes.Structure):
     _fields_ = [
         ("last_kernel_ms", ctypes.c_double),
+        ("last_score_ms", ctypes.c_double),
+        ("last_topk_ms", ctypes.c_double),
         ("last_total_ms", ctypes.c_double),
         ("last_cells", ctypes.c_double),
         ("last_pairs", ctypes.c_int64),

@@ -125,6 +125,10 @@ struct gpusw_ctx {
   int64_t held = 0;
   DevBuf out, meta, queue, ovf, ovf_count, bnd, topk_idx, topk_sc, flush;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
+  // stage markers: pairs (begin, end) of scoring and of top-k launches within one call
+  std::vector<cudaEvent_t> pool;
+  std::vector<std::pair<int, int>> score_marks, topk_marks;
+  int pool_used = 0;
   gpusw_stats st{};
 };
 
@@ -496,8 +500,42 @@ int choose_width(gpusw_ctx* c, int dtype, int max_n, int max_m) {
   return width_ok(c->sch, 2, max_n, max_m) ? 2 : 1;
 }
 
+cudaEvent_t mark(gpusw_ctx* c, int* id) {
+  if (c->pool_used == (int)c->pool.size()) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    c->pool.push_back(e);
+  }
+  *id = c->pool_used++;
+  CK(cudaEventRecord(c->pool[*id], c->stream));
+  return c->pool[*id];
+}
+
+// Bracket the launches issued by f() with a pair of stage events.
+template <class F>
+void staged(gpusw_ctx* c, std::vector<std::pair<int, int>>& marks, F&& f) {
+  int a = 0, b = 0;
+  mark(c, &a);
+  f();
+  mark(c, &b);
+  marks.emplace_back(a, b);
+}
+
+double sum_marks(gpusw_ctx* c, const std::vector<std::pair<int, int>>& marks) {
+  double ms = 0;
+  for (auto& ab : marks) {
+    float x = 0;
+    CK(cudaEventElapsedTime(&x, c->pool[ab.first], c->pool[ab.second]));
+    ms += x;
+  }
+  return ms;
+}
+
 void begin_call(gpusw_ctx* c) {
   set_device(c);
+  c->pool_used = 0;
+  c->score_marks.clear();
+  c->topk_marks.clear();
   c->st.last_launches = 0;
   c->st.last_overflow = 0;
   c->st.last_pairs = 0;
@@ -512,6 +550,8 @@ void end_call(gpusw_ctx* c) {
   CK(cudaEventElapsedTime(&t, c->ev0, c->ev3));
   c->st.last_kernel_ms = k;
   c->st.last_total_ms = t;
+  c->st.last_score_ms = sum_marks(c, c->score_marks);
+  c->st.last_topk_ms = sum_marks(c, c->topk_marks);
   c->st.total_launches += c->st.last_launches;
   c->st.total_overflow += c->st.last_overflow;
   c->st.device_bytes = c->held;
@@ -622,6 +662,7 @@ void gpusw_ctx_destroy(gpusw_ctx* c) {
   if (c->sub_d) cudaFree(c->sub_d);
   for (cudaEvent_t e : {c->ev0, c->ev1, c->ev2, c->ev3})
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -761,14 +802,15 @@ int gpusw_score_cross(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qli
     int P = choose_width(c, dtype, max_n, r.max_len);
     int* d_out = c->out.as<int>(total);
     CK(cudaEventRecord(c->ev1, c->stream));
-    run_cross(c, q, r, qlist, nq, P, d_out, r.n);
+    staged(c, c->score_marks, [&] { run_cross(c, q, r, qlist, nq, P, d_out, r.n); });
     CK(cudaEventRecord(c->ev2, c->stream));
     if (P == 2 && total > 0) {
       const int n_ovf = read_overflow_count(c);
       c->st.last_overflow = n_ovf;
       if (n_ovf > kOvfCap) {  // too many to rescore one by one: redo everything in int32
+        c->score_marks.clear();
         CK(cudaEventRecord(c->ev1, c->stream));
-        run_cross(c, q, r, qlist, nq, 1, d_out, r.n);
+        staged(c, c->score_marks, [&] { run_cross(c, q, r, qlist, nq, 1, d_out, r.n); });
         CK(cudaEventRecord(c->ev2, c->stream));
       }
     }
@@ -811,15 +853,18 @@ int gpusw_topk(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qlist, int
       int* d_sc = c->topk_sc.as<int>((size_t)nq * kk);
       for (int b0 = 0; b0 < nq; b0 += qb) {
         const int nb = std::min(qb, nq - b0);
-        run_cross(c, q, r, qlist + b0, nb, P, d_out, r.n);
+        staged(c, c->score_marks, [&] { run_cross(c, q, r, qlist + b0, nb, P, d_out, r.n); });
         if (P == 2) {
           const int n_ovf = read_overflow_count(c);
           c->st.last_overflow += n_ovf;
-          if (n_ovf > kOvfCap) run_cross(c, q, r, qlist + b0, nb, 1, d_out, r.n);
+          if (n_ovf > kOvfCap)
+            staged(c, c->score_marks, [&] { run_cross(c, q, r, qlist + b0, nb, 1, d_out, r.n); });
         }
-        gsw::topk_kernel<<<nb, 256, 0, c->stream>>>(d_out, r.n, r.n, kk, d_idx + (size_t)b0 * kk,
-                                                     d_sc + (size_t)b0 * kk, kk);
-        CK(cudaGetLastError());
+        staged(c, c->topk_marks, [&] {
+          gsw::topk_kernel<<<nb, 256, 0, c->stream>>>(d_out, r.n, r.n, kk, d_idx + (size_t)b0 * kk,
+                                                       d_sc + (size_t)b0 * kk, kk);
+          CK(cudaGetLastError());
+        });
         c->st.last_launches++;
         if (c->plain) {
           CK(cudaMemcpyAsync(out_idx + (size_t)b0 * kk, d_idx + (size_t)b0 * kk, (size_t)nb * kk * 4, cudaMemcpyDeviceToHost, c->stream));
@@ -923,11 +968,11 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
       if (Pw == 2) launch_overflow_rescore(c, q, r, d_out, queues + slot++);
     };
     if (n > 0) {
-      run(P);
+      staged(c, c->score_marks, [&] { run(P); });
       if (P == 2) {
         const int n_ovf = read_overflow_count(c);
         c->st.last_overflow = n_ovf;
-        if (n_ovf > kOvfCap) run(1);
+        if (n_ovf > kOvfCap) staged(c, c->score_marks, [&] { run(1); });
       }
     }
     CK(cudaEventRecord(c->ev2, c->stream));

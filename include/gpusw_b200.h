@@ -54,6 +54,8 @@ typedef struct gpusw_ctx gpusw_ctx;
  * recorded on the context's stream. */
 typedef struct gpusw_stats {
   double last_kernel_ms;      /* scoring + rescoring + top-k kernels of the last call */
+  double last_score_ms;       /* scoring + int32 rescoring kernels only */
+  double last_topk_ms;        /* top-k kernels only */
   double last_total_ms;       /* the last call's device work including its copies */
   double last_cells;          /* DP cells of the last call (sum of |q| * |r|) */
   int64_t last_pairs;         /* alignments scored by the last call */

@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--nq", type=int, default=None, help="queries (default: the workload's)")
+    ap.add_argument("--nr", type=int, default=None, help="references (default: the workload's)")
     return ap.parse_args()
 
 
@@ -96,10 +98,18 @@ class Group:
             self.dist.destroy_process_group()
 
 
-def workload(name: str):
+def workload(name: str, nq=None, nr=None):
     from gpusw_b200 import workloads
 
-    return workloads.by_name(name)
+    kw = {}
+    if name in ("16s", "protein"):
+        if nq:
+            kw["n_queries"] = nq
+        if nr:
+            kw["n_refs"] = nr
+    elif name == "pairs" and nq:
+        kw["n"] = nq
+    return workloads.by_name(name, **kw)
 
 
 class ClockSampler:
@@ -225,7 +235,7 @@ def run_reference(args, rank):
     threads, each step a bounded seeded sample of the workload."""
     if rank != 0:
         return
-    wl = workload(args.workload)
+    wl = workload(args.workload, args.nq, args.nr)
     per_step = []
     threads = os.cpu_count() or 1
     sample_desc = ""
@@ -259,7 +269,7 @@ def run_ours(args, rank, world, local):
     from gpusw_b200 import _native
 
     group = Group(world)
-    wl = workload(args.workload)
+    wl = workload(args.workload, args.nq, args.nr)
     ctx = _native.context(local)
     ctx.set_scheme(wl.scheme)
     qdb = ctx.upload(*wl.queries)

@@ -344,3 +344,117 @@ __device__ __forceinline__ int finish_score(const SchemeDev& S, const Acc& a, in
 }
 
 }  // namespace gsw
+
+namespace gsw {
+
+// Stream bytes: one residue code per byte, bit 7 set on the last row of a sequence;
+// kStreamPad pads both ends of every team stream (and stands for "no row").
+constexpr int kStreamPadLen = 32;
+
+// Local mode, one column pass over a *stream* of row sequences. The team's rows are
+// concatenated; lane L works on stream row g = t - L at step t, reads its own code byte,
+// and when a row carries the last-row flag it folds its running max into the sequence's
+// partial slot and resets its column state, so the next sequence starts with the row-0
+// boundary while lanes to its right still finish the previous one. The skew of G - 1
+// steps is paid once per stream instead of once per sequence.
+//
+// Rows before a lane's first row and after the stream's end read the pad code, whose
+// profile row scores every column at s_pad <= 0: from the row-0 state such a row leaves
+// H = 0 and F = go, which scores the next real row exactly like F = -inf, so no
+// per-step bounds checks are needed.
+//
+// codes    : stream bytes, codes[-G .. total + G) addressable (pads on both sides).
+// part     : shared, part[slot * G + lane] = running max (HGO units) of sequence `slot`;
+//            max-merged across column passes.
+// bnd      : multi-pass boundary (E, X + go) per stream row, addressable from -G.
+template <int G, int W, int P>
+__device__ __forceinline__ void team_stream_local(const SchemeDev& S, const uint4* __restrict__ prof,
+                                                  int pstride, const int8_t* __restrict__ codes,
+                                                  int total, uint2* bnd, bool has_prev,
+                                                  bool has_next, int lane, unsigned wmask,
+                                                  uint32_t* part) {
+  using Ops = V<P>;
+  const uint32_t GO = Ops::splat(S.go), GE = Ops::splat(S.ge), GES = Ops::splat(S.ges);
+  const uint32_t NEGF = Ops::splat(S.neg_f), NEGE0 = Ops::splat(S.neg_e0);
+  uint32_t HGO[W], F[W];
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    HGO[k] = GO;
+    F[k] = NEGF;
+  }
+  uint32_t hgo_left = GO, best = GO;
+  uint32_t e_out = NEGE0, x_out = GO;
+  int slot = 0;
+  const int8_t* cp = codes - lane;
+  int8_t cb_next = cp[0];
+  const int nsteps = total + G - 1;
+  for (int t = 0; t < nsteps; ++t) {
+    const int8_t cb = cb_next;
+    cb_next = cp[t + 1];
+    uint32_t e_in = __shfl_up_sync(wmask, e_out, 1, G);
+    uint32_t x_in = __shfl_up_sync(wmask, x_out, 1, G);
+    if (lane == 0) {
+      if (has_prev) {
+        const uint2 b = bnd[t];
+        e_in = b.x;
+        x_in = b.y;
+      } else {
+        e_in = NEGE0;
+        x_in = GO;
+      }
+    }
+    const int code = cb & 0x7F;
+    const uint4* pr = prof + code * pstride + lane;
+    constexpr int CH = (W % 16 == 0) ? 16 : ((W % 8 == 0) ? 8 : 4);
+    uint32_t diag = hgo_left;
+    uint32_t e = Ops::addmax(e_in, GES, x_in);
+    hgo_left = Ops::addmax(e_in, GO, x_in);
+    uint32_t xlast = 0;
+#pragma unroll
+    for (int c0 = 0; c0 < W; c0 += CH) {
+      uint32_t sp[CH];
+#pragma unroll
+      for (int k4 = 0; k4 < CH / 4; ++k4) {
+        const uint4 a = pr[(c0 / 4 + k4) * G];
+        sp[4 * k4 + 0] = a.x;
+        sp[4 * k4 + 1] = a.y;
+        sp[4 * k4 + 2] = a.z;
+        sp[4 * k4 + 3] = a.w;
+      }
+      uint32_t XG[CH];
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        const uint32_t f = Ops::addmax(F[c0 + k], GE, HGO[c0 + k]);
+        F[c0 + k] = f;
+        const uint32_t x = Ops::addmax_relu(diag, sp[k], f);
+        diag = HGO[c0 + k];
+        XG[k] = Ops::add(x, GO);
+      }
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        HGO[c0 + k] = Ops::addmax(e, GO, XG[k]);
+        if (c0 + k + 1 < W) e = Ops::addmax(e, GES, XG[k]);
+      }
+      xlast = XG[CH - 1];
+    }
+    e_out = e;
+    x_out = xlast;
+#pragma unroll
+    for (int k = 0; k + 1 < W; k += 2) best = Ops::max3(best, HGO[k], HGO[k + 1]);
+    if (has_next && lane == G - 1) bnd[t - (G - 1)] = make_uint2(e_out, x_out);
+    if (cb < 0) {  // last row of a sequence: fold the partial max, reset to row 0
+      uint32_t* ps = part + slot * G + lane;
+      *ps = Ops::max2(*ps, best);
+      ++slot;
+      best = GO;
+      hgo_left = GO;
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        HGO[k] = GO;
+        F[k] = NEGF;
+      }
+    }
+  }
+}
+
+}  // namespace gsw

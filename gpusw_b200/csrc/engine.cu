@@ -76,6 +76,15 @@ struct Db {
   int* perm_d = nullptr;
   int* ident_d = nullptr;      // identity order (plain form)
   int64_t bytes = 0;
+  // stream buffers (bytes + per-stream offsets/totals), keyed by (plain order, pad code)
+  struct Stream {
+    int8_t* bytes = nullptr;
+    long long* off = nullptr;
+    int* total = nullptr;
+    int n_streams = 0, max_total = 0;
+    int64_t nbytes = 0;
+  };
+  std::vector<std::pair<std::pair<int, int>, Stream>> streams;
   gsw::Packed packed() const {
     gsw::Packed p;
     p.words = words;
@@ -101,6 +110,11 @@ struct Shape {
 const Shape kCrossShapes[] = {{8, 8}, {16, 8}, {16, 16}, {32, 16}, {32, 32}};
 const Shape kPairShapes[] = {{8, 8}, {16, 8}, {16, 16}, {32, 16}};
 constexpr int kNumCross = sizeof(kCrossShapes) / sizeof(Shape);
+// Local-mode streaming kernel shapes (columns per pass = G * W).
+const Shape kStreamShapes[] = {{8, 4},   {8, 8},   {8, 12},  {8, 16},  {8, 24},
+                               {8, 32},  {16, 16}, {16, 20}, {16, 24}, {16, 32},
+                               {32, 16}, {32, 20}, {32, 24}, {32, 32}};
+constexpr int kNumStream = sizeof(kStreamShapes) / sizeof(Shape);
 constexpr int kNumPair = sizeof(kPairShapes) / sizeof(Shape);
 constexpr size_t kSmemCap = 200 * 1024;
 constexpr int kOvfCap = 1 << 20;
@@ -364,6 +378,210 @@ void launch_overflow_rescore(gpusw_ctx* c, const Db& q, const Db& r, int* out,
   launch_pairs(c, shape, 1, c->sch.mode == gsw::kModeLocal, pp, std::max(q.max_len, r.max_len), true);
 }
 
+// Stream buffer of a reference set in sorted (batched) or input (plain) order.
+const Db::Stream& get_stream(gpusw_ctx* c, Db& r, bool plain) {
+  const int pad = c->sch.ns;
+  const std::pair<int, int> key(plain ? 1 : 0, pad);
+  for (auto& kv : r.streams)
+    if (kv.first == key) return kv.second;
+  Db::Stream st;
+  const int R = gsw::kStreamRows, P = gsw::kStreamPadLen;
+  st.n_streams = (r.n + R - 1) / R;
+  std::vector<long long> off(std::max(1, st.n_streams)), row_dst(std::max(1, r.n));
+  std::vector<int> total(std::max(1, st.n_streams));
+  const std::vector<int>& order = r.perm_desc;
+  std::vector<int> ident;
+  if (plain) {
+    ident.resize(r.n);
+    std::iota(ident.begin(), ident.end(), 0);
+  }
+  const std::vector<int>& ord = plain ? ident : order;
+  long long cur = 0;
+  for (int sidx = 0; sidx < st.n_streams; ++sidx) {
+    cur += P;
+    off[sidx] = cur;
+    int tot = 0;
+    for (int j = sidx * R; j < std::min(r.n, sidx * R + R); ++j) {
+      row_dst[j] = cur + tot;
+      tot += r.len[ord[j]];
+    }
+    total[sidx] = tot;
+    st.max_total = std::max(st.max_total, tot);
+    cur += tot + P;
+  }
+  st.nbytes = std::max(1ll, cur) + (long long)st.n_streams * 12;
+  CK(cudaMalloc(&st.bytes, std::max(1ll, cur)));
+  CK(cudaMalloc(&st.off, std::max(1, st.n_streams) * sizeof(long long)));
+  CK(cudaMalloc(&st.total, std::max(1, st.n_streams) * sizeof(int)));
+  CK(cudaMemsetAsync(st.bytes, pad, std::max(1ll, cur), c->stream));
+  CK(cudaMemcpyAsync(st.off, off.data(), off.size() * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(st.total, total.data(), total.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  if (r.n > 0) {
+    long long* dst_d = nullptr;
+    CK(cudaMalloc(&dst_d, r.n * sizeof(long long)));
+    CK(cudaMemcpyAsync(dst_d, row_dst.data(), r.n * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+    const int threads = 256;
+    const long long blocks = ((long long)r.n * 32 + threads - 1) / threads;
+    gsw::build_stream_kernel<<<(unsigned)blocks, threads, 0, c->stream>>>(r.packed(), plain ? r.ident_d : r.perm_d, r.n, dst_d, st.bytes);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    cudaFree(dst_d);
+  }
+  c->held += st.nbytes;
+  r.streams.emplace_back(key, st);
+  return r.streams.back().second;
+}
+
+template <int G, int W, int P>
+void launch_stream_t(gpusw_ctx* c, gsw::StreamParams prm, int n_streams_max_total, bool multipass) {
+  auto k = gsw::cross_stream_kernel<G, W, P>;
+  const size_t smem = profile_bytes(Shape{G, W}, prm.S.ns);
+  static int configured_dev = -1;
+  static size_t configured_smem = 0;
+  if (configured_dev != c->device || configured_smem < smem) {
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(smem, configured_smem)));
+    configured_smem = std::max(smem, configured_smem);
+    configured_dev = c->device;
+  }
+  int bps = 1;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, 256, smem));
+  long long grid = (long long)c->sms * std::max(1, bps);
+  grid = std::max(1ll, std::min<long long>(grid, prm.n_items));
+  const int nteams = 256 / G;
+  if (multipass) {
+    prm.bnd_strip = n_streams_max_total + 2 * gsw::kStreamPadLen;
+    prm.bnd = c->bnd.as<uint2>((size_t)grid * nteams * prm.bnd_strip);
+  } else {
+    prm.bnd = nullptr;
+    prm.bnd_strip = 0;
+  }
+  k<<<(int)grid, 256, smem, c->stream>>>(prm);
+  CK(cudaGetLastError());
+  c->st.last_launches++;
+}
+
+template <int P>
+void launch_stream_shape(gpusw_ctx* c, int shape, const gsw::StreamParams& prm, int mt, bool mp) {
+  switch (shape) {
+    case 0: launch_stream_t<8, 4, P>(c, prm, mt, mp); break;
+    case 1: launch_stream_t<8, 8, P>(c, prm, mt, mp); break;
+    case 2: launch_stream_t<8, 12, P>(c, prm, mt, mp); break;
+    case 3: launch_stream_t<8, 16, P>(c, prm, mt, mp); break;
+    case 4: launch_stream_t<8, 24, P>(c, prm, mt, mp); break;
+    case 5: launch_stream_t<8, 32, P>(c, prm, mt, mp); break;
+    case 6: launch_stream_t<16, 16, P>(c, prm, mt, mp); break;
+    case 7: launch_stream_t<16, 20, P>(c, prm, mt, mp); break;
+    case 8: launch_stream_t<16, 24, P>(c, prm, mt, mp); break;
+    case 9: launch_stream_t<16, 32, P>(c, prm, mt, mp); break;
+    case 10: launch_stream_t<32, 16, P>(c, prm, mt, mp); break;
+    case 11: launch_stream_t<32, 20, P>(c, prm, mt, mp); break;
+    case 12: launch_stream_t<32, 24, P>(c, prm, mt, mp); break;
+    case 13: launch_stream_t<32, 32, P>(c, prm, mt, mp); break;
+    default: fail(GPUSW_ERR_INVALID, "bad stream kernel shape");
+  }
+}
+
+// Cost of scoring `ncols` columns with a shape, per reference row (lane-steps x ops).
+double stream_cost(const Shape& s, int ncols) {
+  const int npass = (std::max(ncols, 1) + s.cap() - 1) / s.cap();
+  return (double)npass * s.G * (5.5 * s.W + 6.0);
+}
+
+int pick_stream_shape(int ncols, int ns, bool plain_largest) {
+  int best = -1;
+  double bc = 0;
+  for (int i = 0; i < kNumStream; ++i) {
+    if (profile_bytes(kStreamShapes[i], ns) > kSmemCap) continue;
+    if (plain_largest) {  // plain form: the widest shape that fits, whatever the lengths
+      best = i;
+      continue;
+    }
+    const double cst = stream_cost(kStreamShapes[i], ncols);
+    if (best < 0 || cst < bc) {
+      best = i;
+      bc = cst;
+    }
+  }
+  return best;
+}
+
+// Local-mode cross product through the streaming kernel (any column length).
+void run_cross_stream(gpusw_ctx* c, const Db& q, Db& r, const int32_t* qlist, int nq, int P,
+                      int* out, long long out_ld) {
+  const HostScheme& h = c->sch;
+  const int nr = r.n;
+  const Db::Stream& st = get_stream(c, r, c->plain != 0);
+  std::vector<int> pos(nq);
+  std::iota(pos.begin(), pos.end(), 0);
+  if (!c->plain)
+    std::stable_sort(pos.begin(), pos.end(), [&](int a, int b) { return q.len[qlist[a]] > q.len[qlist[b]]; });
+  const int npairs = (nq + P - 1) / P;
+  std::vector<int2> pairs(npairs), pair_out(npairs);
+  std::vector<int> pair_cols(npairs);
+  for (int i = 0; i < npairs; ++i) {
+    const int a = pos[i * P];
+    const int b = (P == 2 && i * P + 1 < nq) ? pos[i * P + 1] : -1;
+    pairs[i] = make_int2(qlist[a], b >= 0 ? qlist[b] : -1);
+    pair_out[i] = make_int2(a, b);
+    pair_cols[i] = std::max(q.len[qlist[a]], b >= 0 ? q.len[qlist[b]] : 0);
+  }
+  std::vector<std::vector<int>> bins(kNumStream);
+  for (int i = 0; i < npairs; ++i) {
+    const int sh = pick_stream_shape(pair_cols[i], h.ns, c->plain != 0);
+    if (sh < 0) fail(GPUSW_ERR_SCHEME, "substitution table too large for the profile");
+    bins[sh].push_back(i);
+  }
+  Staging stg;
+  const size_t off_pairs = stg.add(pairs.data(), pairs.size() * sizeof(int2));
+  const size_t off_pout = stg.add(pair_out.data(), pair_out.size() * sizeof(int2));
+  struct L { int shape; size_t items_off; int n_items; bool multipass; };
+  std::vector<L> launches;
+  for (int sh = 0; sh < kNumStream; ++sh) {
+    if (bins[sh].empty()) continue;
+    const int nteams = 256 / kStreamShapes[sh].G;
+    const int nchunks = (st.n_streams + nteams - 1) / nteams;
+    bool mp = false;
+    for (int pi : bins[sh]) mp |= pair_cols[pi] > kStreamShapes[sh].cap();
+    std::vector<int2> items;
+    items.reserve((size_t)nchunks * bins[sh].size());
+    for (int ch = 0; ch < nchunks; ++ch)
+      for (int pi : bins[sh]) items.push_back(make_int2(pi, ch));
+    launches.push_back({sh, stg.add(items.data(), items.size() * sizeof(int2)), (int)items.size(), mp});
+  }
+  char* dmeta = stg.upload(c);
+  const int nslots = (int)launches.size() + 2;
+  unsigned long long* queues = c->queue.as<unsigned long long>(nslots);
+  CK(cudaMemsetAsync(queues, 0, nslots * sizeof(unsigned long long), c->stream));
+  if (P == 2) CK(cudaMemsetAsync(c->ovf_count.as<int>(1), 0, sizeof(int), c->stream));
+  gsw::StreamParams sp{};
+  sp.S = make_scheme(h, P);
+  sp.sub = c->sub_d;
+  sp.cols = q.packed();
+  sp.row_len = r.len_d;
+  sp.row_perm = c->plain ? r.ident_d : r.perm_d;
+  sp.n_rows = nr;
+  sp.stream = st.bytes;
+  sp.stream_off = st.off;
+  sp.stream_total = st.total;
+  sp.n_streams = st.n_streams;
+  sp.pairs = reinterpret_cast<const int2*>(dmeta + off_pairs);
+  sp.pair_out = reinterpret_cast<const int2*>(dmeta + off_pout);
+  sp.out = out;
+  sp.out_ld = out_ld;
+  sp.ovf = c->ovf.as<gsw::Ovf>(kOvfCap);
+  sp.ovf_count = c->ovf_count.as<int>(1);
+  sp.ovf_cap = kOvfCap;
+  int slot = 0;
+  for (const L& l : launches) {
+    sp.items = reinterpret_cast<const int2*>(dmeta + l.items_off);
+    sp.n_items = l.n_items;
+    sp.queue = reinterpret_cast<int*>(queues + slot++);
+    if (P == 2) launch_stream_shape<2>(c, l.shape, sp, st.max_total, l.multipass);
+    else launch_stream_shape<1>(c, l.shape, sp, st.max_total, l.multipass);
+  }
+  if (P == 2) launch_overflow_rescore(c, q, r, out, queues + slot++);
+}
+
 // Cross product of the queries `qlist` (a sublist of q) against every sequence of r into
 // out[a * out_ld + ref] for a = position in qlist. P = 2 (int16 pairs) or 1 (int32).
 // Returns the number of queue counters used (device slots at queues[...]).
@@ -373,6 +591,10 @@ void run_cross(gpusw_ctx* c, const Db& q, const Db& r, const int32_t* qlist, int
   const bool local = h.mode == gsw::kModeLocal;
   const int nr = r.n;
   if (nq == 0 || nr == 0) return;
+  if (local && h.ns <= 126) {
+    run_cross_stream(c, q, const_cast<Db&>(r), qlist, nq, P, out, out_ld);
+    return;
+  }
   // column order: longest first (batched) or input order (plain)
   std::vector<int> pos(nq);
   std::iota(pos.begin(), pos.end(), 0);
@@ -650,6 +872,11 @@ void gpusw_ctx_destroy(gpusw_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (auto& kv : c->dbs) {
     Db& d = *kv.second;
+    for (auto& st : d.streams) {
+      cudaFree(st.second.bytes);
+      cudaFree(st.second.off);
+      cudaFree(st.second.total);
+    }
     cudaFree(d.words);
     cudaFree(d.woff_d);
     cudaFree(d.len_d);
@@ -767,6 +994,12 @@ int gpusw_db_free(gpusw_ctx* c, int32_t db) {
     Db& d = get_db(c, db);
     set_device(c);
     CK(cudaStreamSynchronize(c->stream));
+    for (auto& st : d.streams) {
+      cudaFree(st.second.bytes);
+      cudaFree(st.second.off);
+      cudaFree(st.second.total);
+      c->held -= st.second.nbytes;
+    }
     cudaFree(d.words);
     cudaFree(d.woff_d);
     cudaFree(d.len_d);

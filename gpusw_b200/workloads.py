@@ -80,8 +80,12 @@ def _substitute(rng, seq: np.ndarray, rate: float, k: int = 4) -> np.ndarray:
 
 
 def _indels(rng, seq: np.ndarray, rate: float, probs: np.ndarray) -> np.ndarray:
+    return _indels_at(rng, seq, np.flatnonzero(rng.random(seq.shape[0]) < rate), probs)
+
+
+def _indels_at(rng, seq: np.ndarray, sites: np.ndarray, probs: np.ndarray) -> np.ndarray:
+    """Insert or delete 1-3 residues (50/50) at each site."""
     n = seq.shape[0]
-    sites = np.flatnonzero(rng.random(n) < rate)
     if sites.size == 0:
         return seq
     parts = []
@@ -157,13 +161,17 @@ def pairs(seed: int = 3, n: int = 1_000_000) -> Workload:
     rng = np.random.default_rng(seed)
     windows = rng.integers(0, 4, size=(n, 200), dtype=np.uint8)
     starts = rng.integers(0, 51, size=n)
-    reads = []
+    reads = windows[np.arange(n)[:, None], starts[:, None] + np.arange(150)[None, :]]
+    rate = rng.uniform(0.005, 0.02, size=n)[:, None]
+    hit = rng.random(reads.shape) < rate
+    reads = np.where(hit, (reads + rng.integers(1, 4, size=reads.shape, dtype=np.uint8)) % 4,
+                     reads).astype(np.uint8)
+    sites = rng.random(reads.shape) < 0.001
+    seqs = list(reads)
     uni = np.full(4, 0.25)
-    for i in range(n):
-        rd = windows[i, starts[i]:starts[i] + 150]
-        rd = _substitute(rng, rd, float(rng.uniform(0.005, 0.02)))
-        reads.append(_indels(rng, rd, 0.001, uni))
-    q = _pack(reads)
+    for i in np.flatnonzero(sites.any(axis=1)):
+        seqs[i] = _indels_at(rng, reads[i], np.flatnonzero(sites[i]), uni)
+    q = _pack(seqs)
     r = (windows.reshape(-1).copy(), (np.arange(n + 1, dtype=np.int64) * 200).astype(np.int32))
     idx = np.arange(n, dtype=np.int32)
     return Workload("pairs", schemes.DNA_SEMIGLOBAL.replace(dtype="int16"), q, r, pairs=(idx, idx),

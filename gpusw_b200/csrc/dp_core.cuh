@@ -159,13 +159,21 @@ struct Acc {
 // bnd       : boundary column (E, X+go) at column col0-1 for each row, read by lane 0 when
 //             has_prev, written by lane G-1 when has_next (in place: row i is read at step
 //             i and written at step i + G - 1).
-template <int G, int W, int P, bool LOCAL, bool PAIRS>
+//
+// LEFTPAD (semiglobal with both ends free only): every column sequence is right-aligned to
+// the last column of the last pass; the columns in front of it score 0 against every
+// residue, which reproduces the free column-0 boundary exactly (H stays 0, E enters the
+// first real column at go). The query's last column is then register W-1 of lane G-1 in
+// the last pass, so the end-column maximum costs one op per step instead of one per cell,
+// and the end row needs no column mask (the dummy columns hold 0, which the result takes
+// as a floor anyway).
+template <int G, int W, int P, bool LOCAL, bool PAIRS, bool LEFTPAD = false>
 __device__ __forceinline__ void team_pass(const SchemeDev& S, const uint4* __restrict__ prof,
                                           int pstride, const uint32_t* row_w0,
                                           const uint32_t* row_w1, int row_bits, int row_per,
                                           int m0, int m1, int n0, int n1, int col0,
                                           uint2* bnd, bool has_prev, bool has_next, int lane,
-                                          unsigned wmask, Acc& acc) {
+                                          unsigned wmask, Acc& acc, bool last_pass = true) {
   using Ops = V<P>;
   static_assert(W % 4 == 0, "W must be a multiple of 4");
   const uint32_t GO = Ops::splat(S.go), GE = Ops::splat(S.ge), GES = Ops::splat(S.ges);
@@ -228,7 +236,8 @@ __device__ __forceinline__ void team_pass(const SchemeDev& S, const uint4* __res
     const uint4* pr1 = prof + (PAIRS ? (code >> 16) : code) * pstride + lane;
     // Columns in chunks of CH: F, X and X + go (independent across columns), then the
     // E chain (one add-max per column) and the new HGO. Chunking bounds live registers.
-    constexpr int CH = W < 16 ? W : 16;
+    constexpr int CH = (W % 16 == 0) ? 16 : ((W % 8 == 0) ? 8 : 4);
+    static_assert(W % CH == 0, "column chunks must tile W");
     uint32_t diag = hgo_left;
     uint32_t e = Ops::addmax(e_in, GES, x_in);
     hgo_left = Ops::addmax(e_in, GO, x_in);
@@ -276,7 +285,24 @@ __device__ __forceinline__ void team_pass(const SchemeDev& S, const uint4* __res
     for (int k = 0; k + 1 < W; k += 2) acc.best = Ops::max3(acc.best, HGO[k], HGO[k + 1]);
     if (has_next && lane == G - 1) bnd[i] = make_uint2(e_out, x_out);
 
-    if (!LOCAL) {
+    if (LEFTPAD) {
+      // end column = register W-1 of lane G-1 in the last pass; rows past a half's end
+      // are masked out; the end row is taken over all columns.
+      if (last_pass && lane == G - 1) {
+        const uint32_t keep = (i < m0 ? Ops::half_mask(0) : 0u) | (i < m1 ? Ops::half_mask(1) : 0u);
+        acc.endcol = Ops::max2(acc.endcol, (HGO[W - 1] & keep) | (NEGLOW & ~keep));
+      }
+#pragma unroll
+      for (int h = 0; h < P; ++h) {
+        if (i == (h ? m1 : m0) - 1) {
+          const uint32_t hm = Ops::half_mask(h);
+          uint32_t v = acc.endrow;
+#pragma unroll
+          for (int k = 0; k < W; ++k) v = Ops::max2(v, HGO[k]);
+          acc.endrow = (acc.endrow & ~hm) | (v & hm);
+        }
+      }
+    } else if (!LOCAL) {
       if (track_endcol) {
         if (PAIRS && m0 != m1) {
           // Rows past a half's end must not count towards that half's last column.
@@ -308,7 +334,7 @@ __device__ __forceinline__ void team_pass(const SchemeDev& S, const uint4* __res
       }
     }
   }
-  if (track_endcol) {
+  if (!LEFTPAD && track_endcol) {
 #pragma unroll
     for (int h = 0; h < P; ++h) {
       const int nh = h ? n1 : n0;
@@ -316,6 +342,48 @@ __device__ __forceinline__ void team_pass(const SchemeDev& S, const uint4* __res
 #pragma unroll
       for (int k = 0; k < W; ++k)
         if (jbase + k == nh - 1) acc.endcol = (acc.endcol & ~hm) | (CM[k] & hm);
+    }
+  }
+}
+
+// Lane-local profile fill: lane `lane` writes exactly the slots it reads in team_pass
+// (its W columns of the pass, every code row plus the pad row), so no synchronisation
+// with other lanes is needed. `sub` may point to shared memory. pad0/pad1 shift the
+// halves' columns right (LEFTPAD); positions left of a sequence score 0, positions past
+// its end score s_pad.
+template <int G, int W, int P>
+__device__ __forceinline__ void build_profile_lane(const SchemeDev& S, const int* sub,
+                                                   const Packed& cols, int c0, int n0, int pad0,
+                                                   int c1, int n1, int pad1, int col0,
+                                                   uint4* prof, int pstride, int lane) {
+  const int pad_s = S.s_pad - S.go, zero_s = -S.go;
+  int code[2][W];
+#pragma unroll
+  for (int h = 0; h < P; ++h) {
+    const int c = h ? c1 : c0, n = h ? n1 : n0, pd = h ? pad1 : pad0;
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      const int j = col0 + lane * W + k - pd;  // real column, or < 0 (dummy) / >= n (past end)
+      code[h][k] = (c >= 0 && j >= 0 && j < n) ? cols.code(c, j) : (j < 0 ? -1 : -2);
+    }
+  }
+  for (int a = 0; a <= S.ns; ++a) {
+    uint4* row = prof + a * pstride + lane;
+#pragma unroll
+    for (int k4 = 0; k4 < W / 4; ++k4) {
+      uint32_t v[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        int hv[2] = {pad_s, pad_s};
+#pragma unroll
+        for (int h = 0; h < P; ++h) {
+          const int cd = code[h][4 * k4 + e];
+          hv[h] = cd >= 0 ? (a < S.ns ? sub[a * S.ns + cd] - S.go : pad_s)
+                          : (cd == -1 ? (a < S.ns ? zero_s : pad_s) : pad_s);
+        }
+        v[e] = V<P>::pack(hv[0], hv[1]);
+      }
+      row[k4 * G] = make_uint4(v[0], v[1], v[2], v[3]);
     }
   }
 }
@@ -329,6 +397,14 @@ __device__ __forceinline__ uint32_t team_max(uint32_t v, unsigned wmask) {
 }
 
 // Final score of half h from the team-reduced accumulators (HGO units: subtract go).
+template <int P>
+__device__ __forceinline__ int finish_score_leftpad(const SchemeDev& S, const Acc& a, int h, bool* overflow) {
+  const int best = V<P>::get(a.best, h) - S.go;
+  if (P == 2) *overflow = best > S.ovf_limit;
+  const int ec = V<P>::get(a.endcol, h) - S.go, er = V<P>::get(a.endrow, h) - S.go;
+  return max(max(ec, er), 0);
+}
+
 template <int P>
 __device__ __forceinline__ int finish_score(const SchemeDev& S, const Acc& a, int h, bool* overflow) {
   const int best = V<P>::get(a.best, h) - S.go;
@@ -406,6 +482,7 @@ __device__ __forceinline__ void team_stream_local(const SchemeDev& S, const uint
     const int code = cb & 0x7F;
     const uint4* pr = prof + code * pstride + lane;
     constexpr int CH = (W % 16 == 0) ? 16 : ((W % 8 == 0) ? 8 : 4);
+    static_assert(W % CH == 0, "column chunks must tile W");
     uint32_t diag = hgo_left;
     uint32_t e = Ops::addmax(e_in, GES, x_in);
     hgo_left = Ops::addmax(e_in, GO, x_in);

@@ -108,7 +108,8 @@ struct Shape {
   int cap() const { return G * W; }
 };
 const Shape kCrossShapes[] = {{8, 8}, {16, 8}, {16, 16}, {32, 16}, {32, 32}};
-const Shape kPairShapes[] = {{8, 8}, {16, 8}, {16, 16}, {32, 16}};
+const Shape kPairShapes[] = {{8, 8},  {8, 12},  {8, 16},  {8, 20},
+                             {8, 24}, {16, 16}, {16, 24}, {32, 16}};
 constexpr int kNumCross = sizeof(kCrossShapes) / sizeof(Shape);
 // Local-mode streaming kernel shapes (columns per pass = G * W).
 const Shape kStreamShapes[] = {{8, 4},   {8, 8},   {8, 12},  {8, 16},  {8, 24},
@@ -121,6 +122,46 @@ constexpr int kOvfCap = 1 << 20;
 
 int pstride_of(const Shape& s) { return ((s.G * s.W / 4) + 7) & ~7; }
 size_t profile_bytes(const Shape& s, int ns) { return (size_t)(ns + 1) * pstride_of(s) * 16; }
+
+// Everything one launch sequence touches on the device, plus its stage-timing events.
+// The context owns one set for uncached calls; every cached plan owns its own, because a
+// captured CUDA graph keeps the raw pointers.
+struct Bufs {
+  DevBuf meta, queue, ovf, ovf_count, ovf_flag, bnd, out, idx, sc;
+  std::vector<cudaEvent_t> pool;
+  int pool_used = 0;
+  std::vector<std::pair<int, int>> score_marks, topk_marks;
+  bool capturing = false;  // recording a graph: no host copies, events as graph nodes
+  void set_held(int64_t* h) {
+    for (DevBuf* b : {&meta, &queue, &ovf, &ovf_count, &ovf_flag, &bnd, &out, &idx, &sc}) b->held = h;
+  }
+  void release() {
+    for (DevBuf* b : {&meta, &queue, &ovf, &ovf_count, &ovf_flag, &bnd, &out, &idx, &sc}) b->release();
+    for (cudaEvent_t e : pool) cudaEventDestroy(e);
+    pool.clear();
+  }
+  void reset_marks() {
+    pool_used = 0;
+    score_marks.clear();
+    topk_marks.clear();
+  }
+};
+
+// A cached launch plan: the same call (same sets, scheme, width, options and index
+// arrays) replays its CUDA graph instead of planning and launching again.
+struct Plan {
+  std::vector<long long> key;
+  Bufs B;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long last_use = 0;
+  long long launches = 0;
+  ~Plan() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    B.release();
+  }
+};
 
 }  // namespace
 
@@ -137,12 +178,14 @@ struct gpusw_ctx {
   int plain = 0;
   int64_t mem_budget = 4ll << 30;
   int64_t held = 0;
-  DevBuf out, meta, queue, ovf, ovf_count, bnd, topk_idx, topk_sc, flush;
+  Bufs shared;
+  DevBuf flush;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
-  // stage markers: pairs (begin, end) of scoring and of top-k launches within one call
-  std::vector<cudaEvent_t> pool;
-  std::vector<std::pair<int, int>> score_marks, topk_marks;
-  int pool_used = 0;
+  Bufs* last_bufs = nullptr;  // the set whose stage marks the last call used
+  std::vector<std::unique_ptr<Plan>> plans;
+  unsigned long long use_clock = 0;
+  long long scheme_version = 0;
+  int graphs = 1;              // replay cached plans as CUDA graphs
   gpusw_stats st{};
 };
 
@@ -276,9 +319,9 @@ int pair_teams(const Shape& s, int ns) {
   return std::max(1, t);
 }
 
-template <int G, int W, int P, bool L>
-void launch_pairs_t(gpusw_ctx* c, gsw::PairsParams prm, int teams, long long max_rows, bool multipass) {
-  auto k = gsw::pairs_kernel<G, W, P, L>;
+template <int G, int W, int P, bool L, bool LP>
+void launch_pairs_t(gpusw_ctx* c, Bufs& B, gsw::PairsParams prm, int teams, long long max_rows, bool multipass) {
+  auto k = gsw::pairs_kernel<G, W, P, L, LP>;
   const Shape s{G, W};
   const size_t smem = profile_bytes(s, prm.S.ns) * teams;
   static int configured_dev = -1;
@@ -295,7 +338,7 @@ void launch_pairs_t(gpusw_ctx* c, gsw::PairsParams prm, int teams, long long max
   grid = std::max(1ll, std::min(grid, (team_items + teams - 1) / teams));
   if (multipass) {
     const size_t need = (size_t)grid * teams * (size_t)std::max(1ll, max_rows) * sizeof(uint2);
-    prm.bnd = c->bnd.as<uint2>(need / sizeof(uint2));
+    prm.bnd = B.bnd.as<uint2>(need / sizeof(uint2));
     prm.bnd_cap = (int)std::max(1ll, max_rows);
   } else {
     prm.bnd = nullptr;
@@ -306,26 +349,33 @@ void launch_pairs_t(gpusw_ctx* c, gsw::PairsParams prm, int teams, long long max
   c->st.last_launches++;
 }
 
-template <int P, bool L>
-void launch_pairs_shape(gpusw_ctx* c, int shape, const gsw::PairsParams& prm, int teams, long long max_rows, bool mp) {
+template <int P, bool L, bool LP>
+void launch_pairs_shape(gpusw_ctx* c, Bufs& B, int shape, const gsw::PairsParams& prm, int teams, long long max_rows, bool mp) {
   switch (shape) {
-    case 0: launch_pairs_t<8, 8, P, L>(c, prm, teams, max_rows, mp); break;
-    case 1: launch_pairs_t<16, 8, P, L>(c, prm, teams, max_rows, mp); break;
-    case 2: launch_pairs_t<16, 16, P, L>(c, prm, teams, max_rows, mp); break;
-    case 3: launch_pairs_t<32, 16, P, L>(c, prm, teams, max_rows, mp); break;
+    case 0: launch_pairs_t<8, 8, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
+    case 1: launch_pairs_t<8, 12, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
+    case 2: launch_pairs_t<8, 16, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
+    case 3: launch_pairs_t<8, 20, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
+    case 4: launch_pairs_t<8, 24, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
+    case 5: launch_pairs_t<16, 16, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
+    case 6: launch_pairs_t<16, 24, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
+    case 7: launch_pairs_t<32, 16, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
     default: fail(GPUSW_ERR_INVALID, "bad pairs kernel shape");
   }
 }
 
-void launch_pairs(gpusw_ctx* c, int shape, int P, bool local, const gsw::PairsParams& prm,
+void launch_pairs(gpusw_ctx* c, Bufs& B, int shape, int P, bool local, const gsw::PairsParams& prm,
                   long long max_rows, bool multipass) {
   const int teams = pair_teams(kPairShapes[shape], prm.S.ns);
+  const bool lp = prm.S.mode == gsw::kModeSemi && prm.S.free_q && prm.S.free_r;
   if (P == 2) {
-    if (local) launch_pairs_shape<2, true>(c, shape, prm, teams, max_rows, multipass);
-    else launch_pairs_shape<2, false>(c, shape, prm, teams, max_rows, multipass);
+    if (local) launch_pairs_shape<2, true, false>(c, B, shape, prm, teams, max_rows, multipass);
+    else if (lp) launch_pairs_shape<2, false, true>(c, B, shape, prm, teams, max_rows, multipass);
+    else launch_pairs_shape<2, false, false>(c, B, shape, prm, teams, max_rows, multipass);
   } else {
-    if (local) launch_pairs_shape<1, true>(c, shape, prm, teams, max_rows, multipass);
-    else launch_pairs_shape<1, false>(c, shape, prm, teams, max_rows, multipass);
+    if (local) launch_pairs_shape<1, true, false>(c, B, shape, prm, teams, max_rows, multipass);
+    else if (lp) launch_pairs_shape<1, false, true>(c, B, shape, prm, teams, max_rows, multipass);
+    else launch_pairs_shape<1, false, false>(c, B, shape, prm, teams, max_rows, multipass);
   }
 }
 
@@ -352,15 +402,17 @@ struct Staging {
     if (bytes) memcpy(host.data() + off, src, bytes);
     return off;
   }
-  char* upload(gpusw_ctx* c) {
-    char* d = static_cast<char*>(c->meta.get(std::max<size_t>(host.size(), 256)));
-    if (!host.empty()) CK(cudaMemcpyAsync(d, host.data(), host.size(), cudaMemcpyHostToDevice, c->stream));
+  char* upload(gpusw_ctx* c, Bufs& B) {
+    char* d = static_cast<char*>(B.meta.get(std::max<size_t>(host.size(), 256)));
+    // while recording a graph the plan's metadata is already in place from its eager run
+    if (!host.empty() && !B.capturing)
+      CK(cudaMemcpyAsync(d, host.data(), host.size(), cudaMemcpyHostToDevice, c->stream));
     return d;
   }
 };
 
 // Overflow rescoring of the int16 cells flagged by the previous launches (int32, any length).
-void launch_overflow_rescore(gpusw_ctx* c, const Db& q, const Db& r, int* out,
+void launch_overflow_rescore(gpusw_ctx* c, Bufs& B, const Db& q, const Db& r, int* out,
                              unsigned long long* queue_slot) {
   gsw::PairsParams pp{};
   pp.S = make_scheme(c->sch, 1);
@@ -368,14 +420,15 @@ void launch_overflow_rescore(gpusw_ctx* c, const Db& q, const Db& r, int* out,
   pp.cols = q.packed();
   pp.rows = r.packed();
   pp.item_mode = 1;
-  pp.ovf_in = static_cast<const gsw::Ovf*>(c->ovf.p);
-  pp.ovf_in_count = static_cast<const int*>(c->ovf_count.p);
+  pp.ovf_in = static_cast<const gsw::Ovf*>(B.ovf.p);
+  pp.ovf_in_count = static_cast<const int*>(B.ovf_count.p);
+  pp.ovf_flag = B.ovf_flag.as<int>(1);
   pp.ovf_in_cap = kOvfCap;
   pp.queue = queue_slot;
   pp.out = out;
   pp.n_items = kOvfCap;
   const int shape = pick_pair_shape(1 << 30, c->sch.ns);
-  launch_pairs(c, shape, 1, c->sch.mode == gsw::kModeLocal, pp, std::max(q.max_len, r.max_len), true);
+  launch_pairs(c, B, shape, 1, c->sch.mode == gsw::kModeLocal, pp, std::max(q.max_len, r.max_len), true);
 }
 
 // Stream buffer of a reference set in sorted (batched) or input (plain) order.
@@ -433,7 +486,7 @@ const Db::Stream& get_stream(gpusw_ctx* c, Db& r, bool plain) {
 }
 
 template <int G, int W, int P>
-void launch_stream_t(gpusw_ctx* c, gsw::StreamParams prm, int n_streams_max_total, bool multipass) {
+void launch_stream_t(gpusw_ctx* c, Bufs& B, gsw::StreamParams prm, int n_streams_max_total, bool multipass) {
   auto k = gsw::cross_stream_kernel<G, W, P>;
   const size_t smem = profile_bytes(Shape{G, W}, prm.S.ns);
   static int configured_dev = -1;
@@ -450,7 +503,7 @@ void launch_stream_t(gpusw_ctx* c, gsw::StreamParams prm, int n_streams_max_tota
   const int nteams = 256 / G;
   if (multipass) {
     prm.bnd_strip = n_streams_max_total + 2 * gsw::kStreamPadLen;
-    prm.bnd = c->bnd.as<uint2>((size_t)grid * nteams * prm.bnd_strip);
+    prm.bnd = B.bnd.as<uint2>((size_t)grid * nteams * prm.bnd_strip);
   } else {
     prm.bnd = nullptr;
     prm.bnd_strip = 0;
@@ -461,22 +514,22 @@ void launch_stream_t(gpusw_ctx* c, gsw::StreamParams prm, int n_streams_max_tota
 }
 
 template <int P>
-void launch_stream_shape(gpusw_ctx* c, int shape, const gsw::StreamParams& prm, int mt, bool mp) {
+void launch_stream_shape(gpusw_ctx* c, Bufs& B, int shape, const gsw::StreamParams& prm, int mt, bool mp) {
   switch (shape) {
-    case 0: launch_stream_t<8, 4, P>(c, prm, mt, mp); break;
-    case 1: launch_stream_t<8, 8, P>(c, prm, mt, mp); break;
-    case 2: launch_stream_t<8, 12, P>(c, prm, mt, mp); break;
-    case 3: launch_stream_t<8, 16, P>(c, prm, mt, mp); break;
-    case 4: launch_stream_t<8, 24, P>(c, prm, mt, mp); break;
-    case 5: launch_stream_t<8, 32, P>(c, prm, mt, mp); break;
-    case 6: launch_stream_t<16, 16, P>(c, prm, mt, mp); break;
-    case 7: launch_stream_t<16, 20, P>(c, prm, mt, mp); break;
-    case 8: launch_stream_t<16, 24, P>(c, prm, mt, mp); break;
-    case 9: launch_stream_t<16, 32, P>(c, prm, mt, mp); break;
-    case 10: launch_stream_t<32, 16, P>(c, prm, mt, mp); break;
-    case 11: launch_stream_t<32, 20, P>(c, prm, mt, mp); break;
-    case 12: launch_stream_t<32, 24, P>(c, prm, mt, mp); break;
-    case 13: launch_stream_t<32, 32, P>(c, prm, mt, mp); break;
+    case 0: launch_stream_t<8, 4, P>(c, B, prm, mt, mp); break;
+    case 1: launch_stream_t<8, 8, P>(c, B, prm, mt, mp); break;
+    case 2: launch_stream_t<8, 12, P>(c, B, prm, mt, mp); break;
+    case 3: launch_stream_t<8, 16, P>(c, B, prm, mt, mp); break;
+    case 4: launch_stream_t<8, 24, P>(c, B, prm, mt, mp); break;
+    case 5: launch_stream_t<8, 32, P>(c, B, prm, mt, mp); break;
+    case 6: launch_stream_t<16, 16, P>(c, B, prm, mt, mp); break;
+    case 7: launch_stream_t<16, 20, P>(c, B, prm, mt, mp); break;
+    case 8: launch_stream_t<16, 24, P>(c, B, prm, mt, mp); break;
+    case 9: launch_stream_t<16, 32, P>(c, B, prm, mt, mp); break;
+    case 10: launch_stream_t<32, 16, P>(c, B, prm, mt, mp); break;
+    case 11: launch_stream_t<32, 20, P>(c, B, prm, mt, mp); break;
+    case 12: launch_stream_t<32, 24, P>(c, B, prm, mt, mp); break;
+    case 13: launch_stream_t<32, 32, P>(c, B, prm, mt, mp); break;
     default: fail(GPUSW_ERR_INVALID, "bad stream kernel shape");
   }
 }
@@ -487,15 +540,24 @@ double stream_cost(const Shape& s, int ncols) {
   return (double)npass * s.G * (5.5 * s.W + 6.0);
 }
 
-int pick_stream_shape(int ncols, int ns, bool plain_largest) {
+// Batched form: the shape (and pass count) of least modelled cost for this column length.
+// Plain form: one shape per call -- the smallest single-pass shape that covers the call's
+// longest query, or the widest shape in several passes when none covers it.
+int pick_stream_shape(int ncols, int ns, bool plain) {
   int best = -1;
   double bc = 0;
+  if (plain) {
+    for (int i = 0; i < kNumStream; ++i) {
+      if (profile_bytes(kStreamShapes[i], ns) > kSmemCap) continue;
+      const int cap = kStreamShapes[i].cap(), bcap = best < 0 ? 0 : kStreamShapes[best].cap();
+      const bool covers = cap >= ncols, bcovers = bcap >= ncols;
+      if (best < 0 || (covers && (!bcovers || cap < bcap)) || (!covers && !bcovers && cap > bcap))
+        best = i;
+    }
+    return best;
+  }
   for (int i = 0; i < kNumStream; ++i) {
     if (profile_bytes(kStreamShapes[i], ns) > kSmemCap) continue;
-    if (plain_largest) {  // plain form: the widest shape that fits, whatever the lengths
-      best = i;
-      continue;
-    }
     const double cst = stream_cost(kStreamShapes[i], ncols);
     if (best < 0 || cst < bc) {
       best = i;
@@ -506,7 +568,7 @@ int pick_stream_shape(int ncols, int ns, bool plain_largest) {
 }
 
 // Local-mode cross product through the streaming kernel (any column length).
-void run_cross_stream(gpusw_ctx* c, const Db& q, Db& r, const int32_t* qlist, int nq, int P,
+void run_cross_stream(gpusw_ctx* c, Bufs& B, const Db& q, Db& r, const int32_t* qlist, int nq, int P,
                       int* out, long long out_ld) {
   const HostScheme& h = c->sch;
   const int nr = r.n;
@@ -526,8 +588,9 @@ void run_cross_stream(gpusw_ctx* c, const Db& q, Db& r, const int32_t* qlist, in
     pair_cols[i] = std::max(q.len[qlist[a]], b >= 0 ? q.len[qlist[b]] : 0);
   }
   std::vector<std::vector<int>> bins(kNumStream);
+  const int call_max = npairs ? *std::max_element(pair_cols.begin(), pair_cols.end()) : 0;
   for (int i = 0; i < npairs; ++i) {
-    const int sh = pick_stream_shape(pair_cols[i], h.ns, c->plain != 0);
+    const int sh = pick_stream_shape(c->plain ? call_max : pair_cols[i], h.ns, c->plain != 0);
     if (sh < 0) fail(GPUSW_ERR_SCHEME, "substitution table too large for the profile");
     bins[sh].push_back(i);
   }
@@ -548,11 +611,11 @@ void run_cross_stream(gpusw_ctx* c, const Db& q, Db& r, const int32_t* qlist, in
       for (int pi : bins[sh]) items.push_back(make_int2(pi, ch));
     launches.push_back({sh, stg.add(items.data(), items.size() * sizeof(int2)), (int)items.size(), mp});
   }
-  char* dmeta = stg.upload(c);
+  char* dmeta = stg.upload(c, B);
   const int nslots = (int)launches.size() + 2;
-  unsigned long long* queues = c->queue.as<unsigned long long>(nslots);
+  unsigned long long* queues = B.queue.as<unsigned long long>(nslots);
   CK(cudaMemsetAsync(queues, 0, nslots * sizeof(unsigned long long), c->stream));
-  if (P == 2) CK(cudaMemsetAsync(c->ovf_count.as<int>(1), 0, sizeof(int), c->stream));
+  if (P == 2) CK(cudaMemsetAsync(B.ovf_count.as<int>(1), 0, sizeof(int), c->stream));
   gsw::StreamParams sp{};
   sp.S = make_scheme(h, P);
   sp.sub = c->sub_d;
@@ -568,31 +631,31 @@ void run_cross_stream(gpusw_ctx* c, const Db& q, Db& r, const int32_t* qlist, in
   sp.pair_out = reinterpret_cast<const int2*>(dmeta + off_pout);
   sp.out = out;
   sp.out_ld = out_ld;
-  sp.ovf = c->ovf.as<gsw::Ovf>(kOvfCap);
-  sp.ovf_count = c->ovf_count.as<int>(1);
+  sp.ovf = B.ovf.as<gsw::Ovf>(kOvfCap);
+  sp.ovf_count = B.ovf_count.as<int>(1);
   sp.ovf_cap = kOvfCap;
   int slot = 0;
   for (const L& l : launches) {
     sp.items = reinterpret_cast<const int2*>(dmeta + l.items_off);
     sp.n_items = l.n_items;
     sp.queue = reinterpret_cast<int*>(queues + slot++);
-    if (P == 2) launch_stream_shape<2>(c, l.shape, sp, st.max_total, l.multipass);
-    else launch_stream_shape<1>(c, l.shape, sp, st.max_total, l.multipass);
+    if (P == 2) launch_stream_shape<2>(c, B, l.shape, sp, st.max_total, l.multipass);
+    else launch_stream_shape<1>(c, B, l.shape, sp, st.max_total, l.multipass);
   }
-  if (P == 2) launch_overflow_rescore(c, q, r, out, queues + slot++);
+  if (P == 2) launch_overflow_rescore(c, B, q, r, out, queues + slot++);
 }
 
 // Cross product of the queries `qlist` (a sublist of q) against every sequence of r into
 // out[a * out_ld + ref] for a = position in qlist. P = 2 (int16 pairs) or 1 (int32).
 // Returns the number of queue counters used (device slots at queues[...]).
-void run_cross(gpusw_ctx* c, const Db& q, const Db& r, const int32_t* qlist, int nq, int P,
+void run_cross(gpusw_ctx* c, Bufs& B, const Db& q, const Db& r, const int32_t* qlist, int nq, int P,
                int* out, long long out_ld) {
   const HostScheme& h = c->sch;
   const bool local = h.mode == gsw::kModeLocal;
   const int nr = r.n;
   if (nq == 0 || nr == 0) return;
   if (local && h.ns <= 126) {
-    run_cross_stream(c, q, const_cast<Db&>(r), qlist, nq, P, out, out_ld);
+    run_cross_stream(c, B, q, const_cast<Db&>(r), qlist, nq, P, out, out_ld);
     return;
   }
   // column order: longest first (batched) or input order (plain)
@@ -657,11 +720,11 @@ void run_cross(gpusw_ctx* c, const Db& q, const Db& r, const int32_t* qlist, int
     off_lp = stg.add(long_pairs.data(), long_pairs.size() * sizeof(int2));
     off_lpo = stg.add(long_pout.data(), long_pout.size() * sizeof(int2));
   }
-  char* dmeta = stg.upload(c);
+  char* dmeta = stg.upload(c, B);
   const int nq_slots = (int)launches.size() + 2;
-  unsigned long long* queues = c->queue.as<unsigned long long>(nq_slots);
+  unsigned long long* queues = B.queue.as<unsigned long long>(nq_slots);
   CK(cudaMemsetAsync(queues, 0, nq_slots * sizeof(unsigned long long), c->stream));
-  if (P == 2) CK(cudaMemsetAsync(c->ovf_count.as<int>(1), 0, sizeof(int), c->stream));
+  if (P == 2) CK(cudaMemsetAsync(B.ovf_count.as<int>(1), 0, sizeof(int), c->stream));
   gsw::CrossParams cp{};
   cp.S = make_scheme(h, P);
   cp.sub = c->sub_d;
@@ -673,8 +736,8 @@ void run_cross(gpusw_ctx* c, const Db& q, const Db& r, const int32_t* qlist, int
   cp.n_rows = nr;
   cp.out = out;
   cp.out_ld = out_ld;
-  cp.ovf = c->ovf.as<gsw::Ovf>(kOvfCap);
-  cp.ovf_count = c->ovf_count.as<int>(1);
+  cp.ovf = B.ovf.as<gsw::Ovf>(kOvfCap);
+  cp.ovf_count = B.ovf_count.as<int>(1);
   cp.ovf_cap = kOvfCap;
   int slot = 0;
   for (const Launch& L : launches) {
@@ -702,17 +765,116 @@ void run_cross(gpusw_ctx* c, const Db& q, const Db& r, const int32_t* qlist, int
     pp.ovf = cp.ovf;
     pp.ovf_count = cp.ovf_count;
     pp.ovf_cap = kOvfCap;
-    launch_pairs(c, pick_pair_shape(1 << 30, h.ns), P, local, pp, r.max_len, true);
+    launch_pairs(c, B, pick_pair_shape(1 << 30, h.ns), P, local, pp, r.max_len, true);
   }
-  if (P == 2) launch_overflow_rescore(c, q, r, out, queues + slot++);
+  if (P == 2) launch_overflow_rescore(c, B, q, r, out, queues + slot++);
   (void)row_order;
 }
 
-int read_overflow_count(gpusw_ctx* c) {
+// Largest number of int16 cells flagged by any one launch sequence of the call (read after
+// the call's device work; more than kOvfCap means some were not rescored).
+int read_overflow_count(gpusw_ctx* c, Bufs& B) {
   int n = 0;
-  CK(cudaMemcpyAsync(&n, c->ovf_count.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(&n, B.ovf_flag.as<int>(1), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return n;
+}
+
+// 64-bit hash of a byte range (8-byte words, multiply-xorshift mixing) for plan keys.
+uint64_t fnv1a(const void* data, size_t bytes, uint64_t h = 1469598103934665603ull) {
+  const unsigned char* p = static_cast<const unsigned char*>(data);
+  size_t i = 0;
+  for (; i + 8 <= bytes; i += 8) {
+    uint64_t w;
+    memcpy(&w, p + i, 8);
+    h = (h ^ w) * 0x9E3779B97F4A7C15ull;
+    h ^= h >> 29;
+  }
+  for (; i < bytes; ++i) h = (h ^ p[i]) * 1099511628211ull;
+  return h ^ (uint64_t)bytes;
+}
+
+// Run `body` (the launches of one call) on the shared buffers, or through the plan of `key`:
+// the first time eagerly on the plan's own buffers and then recorded as a CUDA graph,
+// afterwards by replaying the graph. Returns the Bufs that hold the call's results.
+Plan* lookup(gpusw_ctx* c, const std::vector<long long>& key) {
+  if (!c->graphs) return nullptr;
+  for (auto& pl : c->plans)
+    if (pl->key == key) {
+      pl->last_use = ++c->use_clock;
+      return pl.get();
+    }
+  return nullptr;
+}
+
+Bufs& replay(gpusw_ctx* c, Plan* plan) {
+  CK(cudaGraphLaunch(plan->exec, c->stream));
+  c->st.last_launches += plan->launches;
+  return plan->B;
+}
+
+template <class F>
+Bufs& execute(gpusw_ctx* c, const std::vector<long long>& key, bool cacheable, F&& body) {
+  if (!cacheable || !c->graphs) {
+    c->shared.reset_marks();
+    CK(cudaMemsetAsync(c->shared.ovf_flag.as<int>(1), 0, sizeof(int), c->stream));
+    body(c->shared);
+    return c->shared;
+  }
+  if (Plan* hit = lookup(c, key)) return replay(c, hit);
+  Plan* plan = nullptr;
+  if (c->plans.size() >= 4) {  // evict the least recently used plan
+    auto it = std::min_element(c->plans.begin(), c->plans.end(),
+                               [](const auto& a, const auto& b) { return a->last_use < b->last_use; });
+    CK(cudaStreamSynchronize(c->stream));
+    c->plans.erase(it);
+  }
+  c->plans.push_back(std::make_unique<Plan>());
+  plan = c->plans.back().get();
+  plan->key = key;
+  plan->last_use = ++c->use_clock;
+  plan->B.set_held(&c->held);
+  Bufs& B = plan->B;
+  // eager run: allocates every buffer and uploads the plan's metadata
+  B.reset_marks();
+  CK(cudaMemsetAsync(B.ovf_flag.as<int>(1), 0, sizeof(int), c->stream));
+  const long long launches_before = c->st.last_launches;
+  body(B);
+  plan->launches = c->st.last_launches - launches_before;
+  // record the same sequence (no allocation, no host copy) as a graph for later calls
+  CK(cudaStreamSynchronize(c->stream));
+  B.reset_marks();
+  B.capturing = true;
+  cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    try {
+      CK(cudaMemsetAsync(B.ovf_flag.as<int>(1), 0, sizeof(int), c->stream));
+      body(B);
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(c->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      B.capturing = false;
+      throw;
+    }
+    e = cudaStreamEndCapture(c->stream, &plan->graph);
+  }
+  B.capturing = false;
+  c->st.last_launches = launches_before + plan->launches;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&plan->exec, plan->graph, 0);
+  if (e != cudaSuccess) {  // a plan that cannot be recorded is simply not cached
+    cudaGetLastError();
+    c->plans.pop_back();
+    fail(GPUSW_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(e));
+  }
+  return B;
+}
+
+void drop_plans_of(gpusw_ctx* c, int db) {
+  CK(cudaStreamSynchronize(c->stream));
+  c->plans.erase(std::remove_if(c->plans.begin(), c->plans.end(),
+                                [&](const auto& pl) { return pl->key[1] == db || pl->key[2] == db; }),
+                 c->plans.end());
 }
 
 int choose_width(gpusw_ctx* c, int dtype, int max_n, int max_m) {
@@ -722,32 +884,32 @@ int choose_width(gpusw_ctx* c, int dtype, int max_n, int max_m) {
   return width_ok(c->sch, 2, max_n, max_m) ? 2 : 1;
 }
 
-cudaEvent_t mark(gpusw_ctx* c, int* id) {
-  if (c->pool_used == (int)c->pool.size()) {
+int mark(gpusw_ctx* c, Bufs& B) {
+  if (B.pool_used == (int)B.pool.size()) {
     cudaEvent_t e;
     CK(cudaEventCreate(&e));
-    c->pool.push_back(e);
+    B.pool.push_back(e);
   }
-  *id = c->pool_used++;
-  CK(cudaEventRecord(c->pool[*id], c->stream));
-  return c->pool[*id];
+  const int id = B.pool_used++;
+  if (B.capturing) CK(cudaEventRecordWithFlags(B.pool[id], c->stream, cudaEventRecordExternal));
+  else CK(cudaEventRecord(B.pool[id], c->stream));
+  return id;
 }
 
 // Bracket the launches issued by f() with a pair of stage events.
 template <class F>
-void staged(gpusw_ctx* c, std::vector<std::pair<int, int>>& marks, F&& f) {
-  int a = 0, b = 0;
-  mark(c, &a);
+void staged(gpusw_ctx* c, Bufs& B, bool topk, F&& f) {
+  const int a = mark(c, B);
   f();
-  mark(c, &b);
-  marks.emplace_back(a, b);
+  const int b = mark(c, B);
+  (topk ? B.topk_marks : B.score_marks).emplace_back(a, b);
 }
 
-double sum_marks(gpusw_ctx* c, const std::vector<std::pair<int, int>>& marks) {
+double sum_marks(const Bufs& B, const std::vector<std::pair<int, int>>& marks) {
   double ms = 0;
   for (auto& ab : marks) {
     float x = 0;
-    CK(cudaEventElapsedTime(&x, c->pool[ab.first], c->pool[ab.second]));
+    CK(cudaEventElapsedTime(&x, B.pool[ab.first], B.pool[ab.second]));
     ms += x;
   }
   return ms;
@@ -755,9 +917,7 @@ double sum_marks(gpusw_ctx* c, const std::vector<std::pair<int, int>>& marks) {
 
 void begin_call(gpusw_ctx* c) {
   set_device(c);
-  c->pool_used = 0;
-  c->score_marks.clear();
-  c->topk_marks.clear();
+  c->last_bufs = nullptr;
   c->st.last_launches = 0;
   c->st.last_overflow = 0;
   c->st.last_pairs = 0;
@@ -772,8 +932,8 @@ void end_call(gpusw_ctx* c) {
   CK(cudaEventElapsedTime(&t, c->ev0, c->ev3));
   c->st.last_kernel_ms = k;
   c->st.last_total_ms = t;
-  c->st.last_score_ms = sum_marks(c, c->score_marks);
-  c->st.last_topk_ms = sum_marks(c, c->topk_marks);
+  c->st.last_score_ms = c->last_bufs ? sum_marks(*c->last_bufs, c->last_bufs->score_marks) : 0.0;
+  c->st.last_topk_ms = c->last_bufs ? sum_marks(*c->last_bufs, c->last_bufs->topk_marks) : 0.0;
   c->st.total_launches += c->st.last_launches;
   c->st.total_overflow += c->st.last_overflow;
   c->st.device_bytes = c->held;
@@ -848,9 +1008,8 @@ int gpusw_ctx_create(int device, gpusw_ctx** out) {
   }
   auto* c = new gpusw_ctx();
   c->device = device;
-  for (DevBuf* b : {&c->out, &c->meta, &c->queue, &c->ovf, &c->ovf_count, &c->bnd, &c->topk_idx,
-                    &c->topk_sc, &c->flush})
-    b->held = &c->held;
+  c->shared.set_held(&c->held);
+  c->flush.held = &c->held;
   int rc = guarded(c, [&] {
     set_device(c);
     CK(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
@@ -883,13 +1042,12 @@ void gpusw_ctx_destroy(gpusw_ctx* c) {
     cudaFree(d.perm_d);
     cudaFree(d.ident_d);
   }
-  for (DevBuf* b : {&c->out, &c->meta, &c->queue, &c->ovf, &c->ovf_count, &c->bnd, &c->topk_idx,
-                    &c->topk_sc, &c->flush})
-    b->release();
+  c->plans.clear();
+  c->shared.release();
+  c->flush.release();
   if (c->sub_d) cudaFree(c->sub_d);
   for (cudaEvent_t e : {c->ev0, c->ev1, c->ev2, c->ev3})
     if (e) cudaEventDestroy(e);
-  for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -925,6 +1083,7 @@ int gpusw_set_scheme(gpusw_ctx* c, int mode, int go, int ge, int free_q, int fre
     CK(cudaMemcpy(c->sub_d, h.sub.data(), h.sub.size() * sizeof(int), cudaMemcpyHostToDevice));
     c->sch = std::move(h);
     c->has_scheme = true;
+    c->scheme_version++;
   });
 }
 
@@ -993,7 +1152,7 @@ int gpusw_db_free(gpusw_ctx* c, int32_t db) {
   return guarded(c, [&] {
     Db& d = get_db(c, db);
     set_device(c);
-    CK(cudaStreamSynchronize(c->stream));
+    drop_plans_of(c, db);
     for (auto& st : d.streams) {
       cudaFree(st.second.bytes);
       cudaFree(st.second.off);
@@ -1032,22 +1191,31 @@ int gpusw_score_cross(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qli
     }
     begin_call(c);
     const long long total = (long long)nq * r.n;
-    int P = choose_width(c, dtype, max_n, r.max_len);
-    int* d_out = c->out.as<int>(total);
+    const int P = choose_width(c, dtype, max_n, r.max_len);
+    const std::vector<long long> key = {0, qdb, rdb, c->scheme_version, P, c->plain, nq, 0,
+                                        (long long)fnv1a(qlist, (size_t)nq * 4)};
+    auto body = [&](Bufs& B) {
+      int* d_out = B.out.as<int>(total);
+      staged(c, B, false, [&] { run_cross(c, B, q, r, qlist, nq, P, d_out, r.n); });
+    };
     CK(cudaEventRecord(c->ev1, c->stream));
-    staged(c, c->score_marks, [&] { run_cross(c, q, r, qlist, nq, P, d_out, r.n); });
+    Bufs* B = &execute(c, key, total > 0 && !c->plain, body);
     CK(cudaEventRecord(c->ev2, c->stream));
     if (P == 2 && total > 0) {
-      const int n_ovf = read_overflow_count(c);
+      const int n_ovf = read_overflow_count(c, *B);
       c->st.last_overflow = n_ovf;
       if (n_ovf > kOvfCap) {  // too many to rescore one by one: redo everything in int32
-        c->score_marks.clear();
+        c->shared.reset_marks();
         CK(cudaEventRecord(c->ev1, c->stream));
-        staged(c, c->score_marks, [&] { run_cross(c, q, r, qlist, nq, 1, d_out, r.n); });
+        int* d_out = c->shared.out.as<int>(total);
+        staged(c, c->shared, false, [&] { run_cross(c, c->shared, q, r, qlist, nq, 1, d_out, r.n); });
         CK(cudaEventRecord(c->ev2, c->stream));
+        B = &c->shared;
       }
     }
-    if (total > 0) CK(cudaMemcpyAsync(out, d_out, total * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    c->last_bufs = B;
+    if (total > 0)
+      CK(cudaMemcpyAsync(out, B->out.p, total * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaEventRecord(c->ev3, c->stream));
     double rsum = 0;
     for (int l : r.len) rsum += l;
@@ -1075,42 +1243,58 @@ int gpusw_topk(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qlist, int
       qsum += q.len[qlist[a]];
     }
     begin_call(c);
-    CK(cudaEventRecord(c->ev1, c->stream));
     if (nq > 0 && kk > 0) {
-      const int P = choose_width(c, dtype, max_n, r.max_len);
+      int P = choose_width(c, dtype, max_n, r.max_len);
       const long long row_bytes = (long long)r.n * 4;
       int qb = (int)std::max(1ll, std::min<long long>(nq, c->mem_budget / std::max(1ll, row_bytes)));
       if (c->plain) qb = std::min(qb, 16);
-      int* d_out = c->out.as<int>((size_t)qb * r.n);
-      int* d_idx = c->topk_idx.as<int>((size_t)nq * kk);
-      int* d_sc = c->topk_sc.as<int>((size_t)nq * kk);
-      for (int b0 = 0; b0 < nq; b0 += qb) {
-        const int nb = std::min(qb, nq - b0);
-        staged(c, c->score_marks, [&] { run_cross(c, q, r, qlist + b0, nb, P, d_out, r.n); });
-        if (P == 2) {
-          const int n_ovf = read_overflow_count(c);
-          c->st.last_overflow += n_ovf;
-          if (n_ovf > kOvfCap)
-            staged(c, c->score_marks, [&] { run_cross(c, q, r, qlist + b0, nb, 1, d_out, r.n); });
-        }
-        staged(c, c->topk_marks, [&] {
-          gsw::topk_kernel<<<nb, 256, 0, c->stream>>>(d_out, r.n, r.n, kk, d_idx + (size_t)b0 * kk,
-                                                       d_sc + (size_t)b0 * kk, kk);
-          CK(cudaGetLastError());
-        });
-        c->st.last_launches++;
-        if (c->plain) {
-          CK(cudaMemcpyAsync(out_idx + (size_t)b0 * kk, d_idx + (size_t)b0 * kk, (size_t)nb * kk * 4, cudaMemcpyDeviceToHost, c->stream));
-          CK(cudaMemcpyAsync(out_score + (size_t)b0 * kk, d_sc + (size_t)b0 * kk, (size_t)nb * kk * 4, cudaMemcpyDeviceToHost, c->stream));
-          CK(cudaStreamSynchronize(c->stream));
+      auto body_w = [&](int Pw) {
+        return [&, Pw](Bufs& B) {
+          int* d_out = B.out.as<int>((size_t)qb * r.n);
+          int* d_idx = B.idx.as<int>((size_t)nq * kk);
+          int* d_sc = B.sc.as<int>((size_t)nq * kk);
+          for (int b0 = 0; b0 < nq; b0 += qb) {
+            const int nb = std::min(qb, nq - b0);
+            staged(c, B, false, [&] { run_cross(c, B, q, r, qlist + b0, nb, Pw, d_out, r.n); });
+            staged(c, B, true, [&] {
+              gsw::topk_kernel<<<nb, 256, 0, c->stream>>>(d_out, r.n, r.n, kk, d_idx + (size_t)b0 * kk,
+                                                           d_sc + (size_t)b0 * kk, kk);
+              CK(cudaGetLastError());
+              c->st.last_launches++;
+            });
+            if (c->plain && !B.capturing) {  // one batch per call: results back per batch
+              CK(cudaMemcpyAsync(out_idx + (size_t)b0 * kk, d_idx + (size_t)b0 * kk, (size_t)nb * kk * 4,
+                                 cudaMemcpyDeviceToHost, c->stream));
+              CK(cudaMemcpyAsync(out_score + (size_t)b0 * kk, d_sc + (size_t)b0 * kk, (size_t)nb * kk * 4,
+                                 cudaMemcpyDeviceToHost, c->stream));
+              CK(cudaStreamSynchronize(c->stream));
+            }
+          }
+        };
+      };
+      const std::vector<long long> key = {1, qdb, rdb, c->scheme_version, P, c->plain, nq, kk,
+                                          (long long)fnv1a(qlist, (size_t)nq * 4), c->mem_budget};
+      CK(cudaEventRecord(c->ev1, c->stream));
+      Bufs* B = &execute(c, key, !c->plain, body_w(P));
+      CK(cudaEventRecord(c->ev2, c->stream));
+      if (P == 2) {
+        const int n_ovf = read_overflow_count(c, *B);
+        c->st.last_overflow = n_ovf;
+        if (n_ovf > kOvfCap) {  // too many to rescore one by one: redo everything in int32
+          c->shared.reset_marks();
+          CK(cudaEventRecord(c->ev1, c->stream));
+          body_w(1)(c->shared);
+          CK(cudaEventRecord(c->ev2, c->stream));
+          B = &c->shared;
         }
       }
-      CK(cudaEventRecord(c->ev2, c->stream));
+      c->last_bufs = B;
       if (!c->plain) {
-        CK(cudaMemcpyAsync(out_idx, d_idx, (size_t)nq * kk * 4, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaMemcpyAsync(out_score, d_sc, (size_t)nq * kk * 4, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(out_idx, B->idx.p, (size_t)nq * kk * 4, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(out_score, B->sc.p, (size_t)nq * kk * 4, cudaMemcpyDeviceToHost, c->stream));
       }
     } else {
+      CK(cudaEventRecord(c->ev1, c->stream));
       CK(cudaEventRecord(c->ev2, c->stream));
     }
     CK(cudaEventRecord(c->ev3, c->stream));
@@ -1140,76 +1324,111 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
       cells += (double)q.len[qi[i]] * r.len[rj[i]];
     }
     begin_call(c);
-    CK(cudaEventRecord(c->ev1, c->stream));
     const HostScheme& h = c->sch;
     const bool local = h.mode == gsw::kModeLocal;
     int P = n > 0 ? choose_width(c, dtype, max_n, max_m) : 1;
-    int* d_out = c->out.as<int>((size_t)std::max<int64_t>(1, n));
-    auto run = [&](int Pw) {
-      // order: by kernel shape (column length), then row length, then column length
-      std::vector<int> order((size_t)n);
-      std::iota(order.begin(), order.end(), 0);
-      std::vector<int> shp((size_t)n);
-      int plain_shape = 0;
-      if (c->plain) plain_shape = pick_pair_shape(std::max(1, max_n), h.ns);
-      for (int64_t i = 0; i < n; ++i) shp[i] = c->plain ? plain_shape : pick_pair_shape(std::max(1, q.len[qi[i]]), h.ns);
-      if (!c->plain)
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-          if (shp[a] != shp[b]) return shp[a] < shp[b];
-          const int ma = r.len[rj[a]], mb = r.len[rj[b]];
-          if (ma != mb) return ma > mb;
-          return q.len[qi[a]] > q.len[qi[b]];
-        });
-      Staging stg;
-      const size_t o_qi = stg.add(qi, (size_t)n * 4), o_rj = stg.add(rj, (size_t)n * 4);
-      const size_t o_ord = stg.add(order.data(), (size_t)n * 4);
-      char* dm = stg.upload(c);
-      const int nslots = kNumPair + 2;
-      unsigned long long* queues = c->queue.as<unsigned long long>(nslots);
-      CK(cudaMemsetAsync(queues, 0, nslots * sizeof(unsigned long long), c->stream));
-      if (Pw == 2) CK(cudaMemsetAsync(c->ovf_count.as<int>(1), 0, sizeof(int), c->stream));
-      gsw::PairsParams pp{};
-      pp.S = make_scheme(h, Pw);
-      pp.sub = c->sub_d;
-      pp.cols = q.packed();
-      pp.rows = r.packed();
-      pp.qi = reinterpret_cast<const int*>(dm + o_qi);
-      pp.rj = reinterpret_cast<const int*>(dm + o_rj);
-      pp.item_mode = 0;
-      pp.out = d_out;
-      pp.ovf = c->ovf.as<gsw::Ovf>(kOvfCap);
-      pp.ovf_count = c->ovf_count.as<int>(1);
-      pp.ovf_cap = kOvfCap;
-      int64_t i0 = 0;
-      int slot = 0;
-      while (i0 < n) {
-        const int s = shp[order[i0]];
-        int64_t i1 = i0;
-        int mrow = 0, mcol = 0;
-        while (i1 < n && shp[order[i1]] == s) {
-          mrow = std::max(mrow, r.len[rj[order[i1]]]);
-          mcol = std::max(mcol, q.len[qi[order[i1]]]);
-          ++i1;
+    const std::vector<long long> key = {2, qdb, rdb, c->scheme_version, P, c->plain, (long long)n, 0,
+                                        (long long)fnv1a(rj, (size_t)n * 4, fnv1a(qi, (size_t)n * 4))};
+    Bufs* B = nullptr;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    // Plans the call on the host and runs it (recorded as a graph when cacheable).
+    auto plan_and_run = [&](int Pw, bool cacheable) -> Bufs* {
+        // Plan (host, O(n)): kernel shape per alignment from its column length, then a
+        // stable two-pass radix order by (shape, row length descending) so int16x2
+        // partners share a shape and, mostly, a row length.
+        std::vector<int> order((size_t)n);
+        std::vector<uint8_t> shp((size_t)n);
+        const int plain_shape = c->plain ? pick_pair_shape(std::max(1, max_n), h.ns) : 0;
+        {
+          std::vector<int> shape_of_len(4097);
+          for (int L = 0; L <= 4096; ++L) shape_of_len[L] = pick_pair_shape(std::max(1, L), h.ns);
+          const int big = pick_pair_shape(1 << 30, h.ns);
+          std::vector<uint32_t> keyv((size_t)n);
+          for (int64_t i = 0; i < n; ++i) {
+            const int ql = q.len[qi[i]];
+            shp[i] = (uint8_t)(c->plain ? plain_shape : (ql <= 4096 ? shape_of_len[ql] : big));
+            keyv[i] = ((uint32_t)shp[i] << 24) | (0xFFFFFFu - (uint32_t)std::min(r.len[rj[i]], 0xFFFFFF));
+          }
+          if (c->plain) {
+            std::iota(order.begin(), order.end(), 0);
+          } else {
+            std::vector<int> tmp((size_t)n);
+            std::iota(tmp.begin(), tmp.end(), 0);
+            std::vector<int64_t> cnt(65537);
+            for (int pass = 0; pass < 2; ++pass) {
+              const int sh = pass * 16;
+              std::fill(cnt.begin(), cnt.end(), 0);
+              for (int64_t i = 0; i < n; ++i) cnt[((keyv[tmp[i]] >> sh) & 0xFFFF) + 1]++;
+              for (int bkt = 0; bkt < 65536; ++bkt) cnt[bkt + 1] += cnt[bkt];
+              for (int64_t i = 0; i < n; ++i) order[cnt[(keyv[tmp[i]] >> sh) & 0xFFFF]++] = tmp[i];
+              if (pass == 0) tmp.swap(order);
+            }
+          }
         }
-        pp.order = reinterpret_cast<const int*>(dm + o_ord) + i0;
-        pp.n_align = i1 - i0;
-        pp.n_items = (pp.n_align + Pw - 1) / Pw;
-        pp.queue = queues + slot++;
-        launch_pairs(c, s, Pw, local, pp, mrow, mcol > kPairShapes[s].cap());
-        i0 = i1;
-      }
-      if (Pw == 2) launch_overflow_rescore(c, q, r, d_out, queues + slot++);
+        struct Bin { int64_t i0, i1; int shape, mrow, mcol; };
+        std::vector<Bin> plan_bins;
+        for (int64_t i0 = 0; i0 < n;) {
+          const int sh = shp[order[i0]];
+          int64_t i1 = i0;
+          int mrow = 0, mcol = 0;
+          while (i1 < n && shp[order[i1]] == sh) {
+            mrow = std::max(mrow, r.len[rj[order[i1]]]);
+            mcol = std::max(mcol, q.len[qi[order[i1]]]);
+            ++i1;
+          }
+          plan_bins.push_back({i0, i1, sh, mrow, mcol});
+          i0 = i1;
+        }
+        Staging stg;
+        const size_t o_qi = stg.add(qi, (size_t)n * 4), o_rj = stg.add(rj, (size_t)n * 4);
+        const size_t o_ord = stg.add(order.data(), (size_t)n * 4);
+        auto run = [&](int Pw) {
+          return [&, Pw](Bufs& Bx) {
+            char* dm = stg.upload(c, Bx);
+            int* d_out = Bx.out.as<int>((size_t)n);
+            const int nslots = (int)plan_bins.size() + 2;
+            unsigned long long* queues = Bx.queue.as<unsigned long long>(nslots);
+            staged(c, Bx, false, [&] {
+              CK(cudaMemsetAsync(queues, 0, nslots * sizeof(unsigned long long), c->stream));
+              if (Pw == 2) CK(cudaMemsetAsync(Bx.ovf_count.as<int>(1), 0, sizeof(int), c->stream));
+              gsw::PairsParams pp{};
+              pp.S = make_scheme(h, Pw);
+              pp.sub = c->sub_d;
+              pp.cols = q.packed();
+              pp.rows = r.packed();
+              pp.qi = reinterpret_cast<const int*>(dm + o_qi);
+              pp.rj = reinterpret_cast<const int*>(dm + o_rj);
+              pp.item_mode = 0;
+              pp.out = d_out;
+              pp.ovf = Bx.ovf.as<gsw::Ovf>(kOvfCap);
+              pp.ovf_count = Bx.ovf_count.as<int>(1);
+              pp.ovf_cap = kOvfCap;
+              int slot = 0;
+              for (const Bin& bn : plan_bins) {
+                pp.order = reinterpret_cast<const int*>(dm + o_ord) + bn.i0;
+                pp.n_align = bn.i1 - bn.i0;
+                pp.n_items = (pp.n_align + Pw - 1) / Pw;
+                pp.queue = queues + slot++;
+                launch_pairs(c, Bx, bn.shape, Pw, local, pp, bn.mrow, bn.mcol > kPairShapes[bn.shape].cap());
+              }
+              if (Pw == 2) launch_overflow_rescore(c, Bx, q, r, d_out, queues + slot++);
+            });
+          };
+        };
+        return &execute(c, key, cacheable, run(Pw));
     };
     if (n > 0) {
-      staged(c, c->score_marks, [&] { run(P); });
+      Plan* hit = c->plain ? nullptr : lookup(c, key);
+      B = hit ? &replay(c, hit) : plan_and_run(P, !c->plain);
       if (P == 2) {
-        const int n_ovf = read_overflow_count(c);
+        const int n_ovf = read_overflow_count(c, *B);
         c->st.last_overflow = n_ovf;
-        if (n_ovf > kOvfCap) staged(c, c->score_marks, [&] { run(1); });
+        if (n_ovf > kOvfCap) B = plan_and_run(1, false);  // too many flagged cells: all int32
       }
     }
+    c->last_bufs = B;
     CK(cudaEventRecord(c->ev2, c->stream));
-    if (n > 0) CK(cudaMemcpyAsync(out, d_out, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (n > 0) CK(cudaMemcpyAsync(out, B->out.p, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaEventRecord(c->ev3, c->stream));
     c->st.last_cells = cells;
     c->st.last_pairs = n;
@@ -1248,7 +1467,7 @@ int gpusw_measure_dpx_rate(gpusw_ctx* c, double* ops_per_s) {
     unsigned hin[16];
     for (int i = 0; i < 16; ++i) hin[i] = 0x00030005u * (i + 1);
     hin[0] = 0xFFFEFFFEu;
-    unsigned* din = static_cast<unsigned*>(c->meta.get(64 + (size_t)blocks * threads * 4));
+    unsigned* din = static_cast<unsigned*>(c->shared.meta.get(64 + (size_t)blocks * threads * 4));
     unsigned* dout = din + 16;
     CK(cudaMemcpyAsync(din, hin, 64, cudaMemcpyHostToDevice, c->stream));
     for (int w = 0; w < 3; ++w) dpx_rate_kernel<<<blocks, threads, 0, c->stream>>>(din, dout, iters);

@@ -164,6 +164,7 @@ struct PairsParams {
   const Ovf* ovf_in;
   const int* ovf_in_count;
   int ovf_in_cap;
+  int* ovf_flag;             // overflow mode: max of the input counts seen in a call
   const int2* pairs;
   const int2* pair_out;
   const int* row_perm;
@@ -226,18 +227,31 @@ __device__ __forceinline__ PairItem<P> decode_item(const PairsParams& p, long lo
   return it;
 }
 
-template <int G, int W, int P, bool LOCAL>
+constexpr int kSubSmemMax = 64;  // substitution tables up to 64 x 64 are staged in shared memory
+
+template <int G, int W, int P, bool LOCAL, bool LEFTPAD>
 __global__ void __launch_bounds__(256) pairs_kernel(const PairsParams p) {
   extern __shared__ uint4 smem_prof[];
+  __shared__ int s_sub[kSubSmemMax * kSubSmemMax];
   constexpr int SLOTS = G * W / 4;
   const int pstride = (SLOTS + 7) & ~7;
   const int team = threadIdx.x / G, lane = threadIdx.x % G, nteams = blockDim.x / G;
   const unsigned wmask = (G == 32) ? 0xFFFFFFFFu
                                    : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
-  uint4* prof = smem_prof + (size_t)team * (p.S.ns + 1) * pstride;
+  const int ns = p.S.ns;
+  const int* sub = p.sub;
+  if (ns <= kSubSmemMax) {
+    for (int i = threadIdx.x; i < ns * ns; i += blockDim.x) s_sub[i] = p.sub[i];
+    __syncthreads();
+    sub = s_sub;
+  }
+  uint4* prof = smem_prof + (size_t)team * (ns + 1) * pstride;
   uint2* bnd = p.bnd ? p.bnd + ((size_t)blockIdx.x * nteams + team) * p.bnd_cap : nullptr;
   long long n_items = p.n_items;
-  if (p.item_mode == 1) n_items = min(*p.ovf_in_count, p.ovf_in_cap);
+  if (p.item_mode == 1) {
+    n_items = min(*p.ovf_in_count, p.ovf_in_cap);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && p.ovf_flag) atomicMax(p.ovf_flag, *p.ovf_in_count);
+  }
   for (;;) {
     unsigned long long t = 0;
     if (lane == 0) t = atomicAdd(p.queue, 1ull);
@@ -256,17 +270,20 @@ __global__ void __launch_bounds__(256) pairs_kernel(const PairsParams p) {
     Acc acc = init_acc<P>(p.S);
     if (ncols > 0 && mrows > 0) {
       const int npass = (ncols + G * W - 1) / (G * W);
+      const int span = npass * G * W;
+      const int pad0 = LEFTPAD ? span - n0 : 0, pad1 = LEFTPAD ? span - n1 : 0;
       const uint32_t* w0 = p.rows.words + p.rows.woff[max(it.r[0], 0)];
       const uint32_t* w1 = (P == 2 && it.r[P - 1] >= 0) ? p.rows.words + p.rows.woff[it.r[P - 1]] : w0;
       for (int ps = 0; ps < npass; ++ps) {
+        build_profile_lane<G, W, P>(p.S, sub, p.cols, it.valid[0] ? it.q[0] : -1, n0, pad0,
+                                    (P == 2 && it.valid[P - 1]) ? it.q[P - 1] : -1, n1, pad1,
+                                    ps * G * W, prof, pstride, lane);
+        team_pass<G, W, P, LOCAL, true, LEFTPAD>(p.S, prof, pstride, w0, w1, p.rows.bits,
+                                                 p.rows.per, m0, P == 2 ? m1 : m0,
+                                                 LEFTPAD ? span : n0, LEFTPAD ? span : n1,
+                                                 ps * G * W, bnd, ps > 0, ps + 1 < npass, lane,
+                                                 wmask, acc, ps + 1 == npass);
         __syncwarp(wmask);
-        build_profile<G, W, P>(p.S, p.sub, p.cols, it.valid[0] ? it.q[0] : -1, n0,
-                               (P == 2 && it.valid[P - 1]) ? it.q[P - 1] : -1, n1, ps * G * W,
-                               prof, pstride, lane, G);
-        __syncwarp(wmask);
-        team_pass<G, W, P, LOCAL, true>(p.S, prof, pstride, w0, w1, p.rows.bits, p.rows.per,
-                                        m0, P == 2 ? m1 : m0, n0, n1, ps * G * W, bnd, ps > 0,
-                                        ps + 1 < npass, lane, wmask, acc);
       }
       acc = reduce_acc<G, P>(p.S, acc, wmask);
     }
@@ -275,8 +292,10 @@ __global__ void __launch_bounds__(256) pairs_kernel(const PairsParams p) {
       for (int a = 0; a < P; ++a) {
         if (!it.valid[a]) continue;
         bool ovf = false;
-        int score = (n[a] == 0 || m[a] == 0) ? empty_score(p.S, n[a], m[a])
-                                             : finish_score<P>(p.S, acc, a, &ovf);
+        int score;
+        if (n[a] == 0 || m[a] == 0) score = empty_score(p.S, n[a], m[a]);
+        else if (LEFTPAD) score = finish_score_leftpad<P>(p.S, acc, a, &ovf);
+        else score = finish_score<P>(p.S, acc, a, &ovf);
         if (P == 2 && ovf && n[a] > 0 && m[a] > 0) {
           push_overflow(p.ovf, p.ovf_count, p.ovf_cap, it.q[a], it.r[a], it.pos[a]);
           score = INT_MIN;

@@ -1,0 +1,111 @@
+"""Engine behaviour on the GPU: cached plans replayed as CUDA graphs, plan eviction, the
+plain (one-batch-per-call) form, and stats -- every result checked against the oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from gpusw_b200 import Aligner, Scheme, _native, schemes
+from gpusw_b200.encode import funnel
+from tests._util import rand_seqs
+
+pytestmark = pytest.mark.gpu
+
+
+def _sets(seed, nq=21, nr=300, alpha="ACGT", lo=20, hi=400):
+    rng = np.random.default_rng(seed)
+    return rand_seqs(rng, nq, lo, hi, alpha), rand_seqs(rng, nr, lo, hi, alpha)
+
+
+def test_graph_replay_cross_topk_pairs_bitexact():
+    qs, rs = _sets(1)
+    sch = schemes.DNA
+    al = Aligner(sch).index(rs).set_queries(qs)
+    want = oracle.score_cross(funnel(qs, sch), funnel(rs, sch), sch)
+    for _ in range(3):  # first call records the plan, the next ones replay its graph
+        assert np.array_equal(al.score_cross().astype(np.int64), want)
+    idx, sc = oracle.topk_stable(want, 7)
+    for _ in range(3):
+        tk = al.top_k(k=7)
+        assert np.array_equal(tk.topk_idx, idx) and np.array_equal(tk.topk_scores, sc)
+    qi = np.arange(21) % 21
+    rj = (np.arange(21) * 7) % 300
+    for _ in range(3):
+        got = al.score_pairs(qi, rj)
+        assert got.astype(np.int64).tolist() == [int(want[i, j]) for i, j in zip(qi, rj)]
+    st = _native.context(0).stats()
+    assert st.last_launches > 0 and st.last_kernel_ms > 0
+
+
+def test_plan_eviction_and_many_keys():
+    qs, rs = _sets(2, nq=9, nr=120)
+    sch = schemes.DNA
+    al = Aligner(sch).index(rs).set_queries(qs)
+    want = oracle.score_cross(funnel(qs, sch), funnel(rs, sch), sch)
+    for k in (1, 2, 3, 4, 5, 6, 1, 2):  # more keys than cached plans
+        tk = al.top_k(k=k)
+        idx, sc = oracle.topk_stable(want, k)
+        assert np.array_equal(tk.topk_idx, idx) and np.array_equal(tk.topk_scores, sc)
+
+
+def test_scheme_change_invalidates_plans():
+    qs, rs = _sets(3, nq=6, nr=50)
+    a = Aligner(schemes.DNA).index(rs).set_queries(qs)
+    b = Aligner(schemes.DNA_GLOBAL).index(rs).set_queries(qs)
+    for _ in range(2):
+        for al, sch in ((a, schemes.DNA), (b, schemes.DNA_GLOBAL)):
+            want = oracle.score_cross(funnel(qs, sch), funnel(rs, sch), sch)
+            assert np.array_equal(al.score_cross().astype(np.int64), want)
+
+
+@pytest.mark.parametrize("name,alpha", [("dna", "ACGT"), ("blosum62", "ARNDCQEGHILKMFPSTWYV")])
+def test_plain_form_equals_batched(name, alpha):
+    sch = schemes.DNA if name == "dna" else schemes.BLOSUM62
+    qs, rs = _sets(4, nq=37, nr=211, alpha=alpha, lo=5, hi=1300)
+    ctx = _native.context(0)
+    al = Aligner(sch).index(rs).set_queries(qs)
+    batched = al.top_k(k=10)
+    full = al.score_cross()
+    try:
+        ctx.set_options(plain=True)
+        plain = al.top_k(k=10)
+        plain_full = al.score_cross()
+        plain_pairs = al.score_pairs(np.arange(37), np.arange(37))
+    finally:
+        ctx.set_options(plain=False)
+    want = oracle.score_cross(funnel(qs, sch), funnel(rs, sch), sch)
+    assert np.array_equal(full.astype(np.int64), want)
+    assert np.array_equal(plain_full.astype(np.int64), want)
+    assert np.array_equal(plain.topk_idx, batched.topk_idx)
+    assert np.array_equal(plain.topk_scores, batched.topk_scores)
+    assert plain_pairs.astype(np.int64).tolist() == [int(want[i, i]) for i in range(37)]
+
+
+def test_memory_budget_blocks_topk():
+    qs, rs = _sets(5, nq=40, nr=500)
+    sch = schemes.DNA
+    ctx = _native.context(0)
+    al = Aligner(sch).index(rs).set_queries(qs)
+    try:
+        ctx.set_options(plain=False, mem_budget=500 * 4 * 7)  # 7 query rows per block
+        tk = al.top_k(k=5)
+    finally:
+        ctx.set_options(plain=False, mem_budget=0)
+    want = oracle.score_cross(funnel(qs, sch), funnel(rs, sch), sch)
+    idx, sc = oracle.topk_stable(want, 5)
+    assert np.array_equal(tk.topk_idx, idx) and np.array_equal(tk.topk_scores, sc)
+
+
+def test_overflow_rescore_through_graph_replay():
+    sch = Scheme(mode="local", match=300, mismatch=-7, gap_open=-9, gap_extend=-4)
+    rng = np.random.default_rng(8)
+    base = rand_seqs(rng, 1, 150, 151, "ACGT")[0]
+    qs = [base, base[:30]] + rand_seqs(rng, 5, 1, 150, "ACGT")
+    rs = [base] + rand_seqs(rng, 30, 1, 200, "ACGT")
+    al = Aligner(sch).index(rs).set_queries(qs)
+    want = oracle.score_cross(funnel(qs, sch), funnel(rs, sch), sch)
+    assert want.max() > 32767
+    for _ in range(3):
+        assert np.array_equal(al.score_cross().astype(np.int64), want)
+        tk = al.top_k(k=3)
+        idx, sc = oracle.topk_stable(want, 3)
+        assert np.array_equal(tk.topk_idx, idx) and np.array_equal(tk.topk_scores, sc)

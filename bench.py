@@ -50,7 +50,12 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="16s", choices=["16s", "protein", "pairs", "small"])
+    ap.add_argument("--workload", default="16s",
+                    choices=["16s", "protein", "pairs", "small", "serving"])
+    ap.add_argument("--serve-loads", default="1,4,16",
+                    help="offered loads (requests/s) of the serving sweep")
+    ap.add_argument("--serve-requests", type=int, default=8, help="requests per offered load")
+    ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=2)
@@ -235,7 +240,7 @@ def run_reference(args, rank):
     threads, each step a bounded seeded sample of the workload."""
     if rank != 0:
         return
-    wl = workload(args.workload, args.nq, args.nr)
+    wl = workload("16s" if args.workload == "serving" else args.workload, args.nq, args.nr)
     per_step = []
     threads = os.cpu_count() or 1
     sample_desc = ""
@@ -263,6 +268,79 @@ def packed_bytes(offs: np.ndarray, bits: int) -> int:
     lens = np.diff(offs).astype(np.int64)
     words = ((lens + per - 1) // per + 3) // 4 * 4
     return int(words.sum() * 4 + 64 * 4 + lens.shape[0] * 20)
+
+
+def serving_sweep(aligner, loads, n_requests, seed=4, slots=2, k=10):
+    """Poisson request stream at each offered load against the resident references of
+    `aligner`; latencies (submit -> done) and sustained GCUPS come from the native server."""
+    import threading
+
+    from gpusw_b200 import workloads
+    from gpusw_b200.encode import Encoded
+    from gpusw_b200.server import Server
+
+    reqs = workloads.requests(seed=seed, n_requests=n_requests)
+    sch = aligner.scheme
+    encs = [Encoded(c, o, list(range(o.shape[0] - 1)), np.diff(o).astype(np.int32), sch.eff_alphabet)
+            for c, o in reqs]
+    rng = np.random.default_rng(seed + 1)
+    out = []
+    for lam in loads:
+        with Server(aligner, k=k, slots=slots, max_batch_queries=1024) as srv:
+            gaps = rng.exponential(1.0 / lam, size=len(encs))
+            ids, done = [], []
+
+            def collect():
+                while len(done) < len(encs):
+                    if not ids:
+                        time.sleep(0.001)
+                        continue
+                    rid = ids.pop(0)
+                    srv.result(rid, timeout=900)
+                    done.append(rid)
+
+            t0 = time.perf_counter()
+            th = threading.Thread(target=collect)
+            th.start()
+            t_next = t0
+            for e, g in zip(encs, gaps):
+                t_next += g
+                delay = t_next - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                rid = srv.submit(e)
+                ids.append(rid)
+            th.join(timeout=1800)
+            st = srv.stats()
+        out.append({"offered_rps": lam, "requests": len(encs), "completed": st["completed"],
+                    "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                    "max_ms": st["max_ms"], "gcups": st["gcups"],
+                    "achieved_rps": st["completed"] / st["wall_s"] if st["wall_s"] else None,
+                    "batches": st["batches"], "mean_batch_queries": st["mean_batch_queries"]})
+    return out
+
+
+def run_serving(args, rank, world, local):
+    """--workload serving: the serving sweep alone (16S reference set resident)."""
+    from gpusw_b200 import Aligner
+    from gpusw_b200.encode import Encoded
+
+    wl = workload("16s", None, args.nr)
+    refs = Encoded(wl.refs[0], wl.refs[1], list(range(wl.nr)), np.diff(wl.refs[1]).astype(np.int32),
+                   wl.scheme.eff_alphabet)
+    al = Aligner(wl.scheme, device=local).index(refs)
+    loads = [float(x) for x in args.serve_loads.split(",")]
+    sweep = serving_sweep(al, loads, args.serve_requests)
+    if rank == 0:
+        top = max(sweep, key=lambda r: r["gcups"])
+        print(json.dumps({"metric": METRIC, "value": top["gcups"], "unit": "GCUPS", "n_gpus": world,
+                          "steps": len(sweep), "warmup": 0, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "int16x2 (int32 rescoring)",
+                          "data": "synthetic",
+                          "config": {"workload": "serving over the resident 16S reference set, top-10",
+                                     "refs": wl.nr, "requests_per_load": args.serve_requests,
+                                     "request_queries": "1-512 log-uniform, lengths U[50,2000]"},
+                          "serving": sweep}), flush=True)
 
 
 def run_ours(args, rank, world, local):
@@ -354,6 +432,19 @@ def run_ours(args, rank, world, local):
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "timing": "wall clock around upload + score + top-k + copy back"}
 
+    # a short serving sweep over the same resident references (16S workload only)
+    serving = None
+    if wl.name == "16s" and not args.no_serve and args.serve_requests > 0:
+        from gpusw_b200 import Aligner
+        from gpusw_b200.encode import Encoded
+
+        refs = Encoded(wl.refs[0], wl.refs[1], list(range(wl.nr)),
+                       np.diff(wl.refs[1]).astype(np.int32), wl.scheme.eff_alphabet)
+        al = Aligner(wl.scheme, device=local).index(refs)
+        serving = serving_sweep(al, [float(x) for x in args.serve_loads.split(",")],
+                                args.serve_requests)
+        del al
+
     # CPU oracle baseline and a bit-exact check of the same sample (rank 0, N = 1)
     cpu = None
     bitexact = None
@@ -402,7 +493,7 @@ def run_ours(args, rank, world, local):
                             "topk_ms_per_step": sum(topk_ms) / args.steps},
                "plain": plain, "batched_over_plain": (value / plain["value"]) if plain else None,
                "e2e": e2e, "cpu_baseline": cpu, "bitexact_sample": bitexact,
-               "overflow_rescored": ovf, "clocks": clocks}
+               "overflow_rescored": ovf, "serving": serving, "clocks": clocks}
         print(json.dumps(out), flush=True)
     group.close()
 
@@ -412,6 +503,9 @@ def main():
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload == "serving":
+        run_serving(args, rank, world, local)
         return
     run_ours(args, rank, world, local)
 

@@ -15,7 +15,7 @@ import numpy as np
 
 from .errors import GpuSWError, NoGpuError, OverflowRiskError, SchemeError
 
-__all__ = ["LIB_PATH", "load", "gpu_available", "Context", "context", "Stats"]
+__all__ = ["LIB_PATH", "load", "gpu_available", "Context", "context", "Stats", "ServerStats"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libgpusw_sm100.so")
 
@@ -44,6 +44,21 @@ class Stats(ctypes.Structure):
     ]
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_int64), ("completed", ctypes.c_int64),
+        ("cancelled", ctypes.c_int64), ("rejected", ctypes.c_int64),
+        ("pending", ctypes.c_int64), ("running", ctypes.c_int64),
+        ("batches", ctypes.c_int64), ("mean_batch_queries", ctypes.c_double),
+        ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+        ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
+        ("cells", ctypes.c_double), ("wall_s", ctypes.c_double), ("gcups", ctypes.c_double),
+        ("device_bytes", ctypes.c_int64),
+    ]
+
+
+_VP, _I32, _I64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+
 _SIGNATURES = {
     "gpusw_version": ([], ctypes.c_int),
     "gpusw_device_count": ([ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
@@ -69,6 +84,14 @@ _SIGNATURES = {
     "gpusw_sync": ([ctypes.c_void_p], ctypes.c_int),
     "gpusw_measure_dpx_rate": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "gpusw_flush_l2": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+    "gpusw_server_create": ([_VP, _I32, _I32, ctypes.c_int, _I64, _I32, _I32, _I32,
+                             ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "gpusw_server_submit": ([_VP, _VP, _VP, _I32, ctypes.POINTER(_I64)], ctypes.c_int),
+    "gpusw_server_poll": ([_VP, _I64, _I32, ctypes.POINTER(_I32), _VP, _VP], ctypes.c_int),
+    "gpusw_server_cancel": ([_VP, _I64], ctypes.c_int),
+    "gpusw_server_get_stats": ([_VP, ctypes.POINTER(ServerStats)], ctypes.c_int),
+    "gpusw_server_last_error": ([_VP], ctypes.c_char_p),
+    "gpusw_server_destroy": ([_VP], None),
 }
 
 

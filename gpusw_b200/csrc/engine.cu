@@ -1493,3 +1493,4 @@ int gpusw_flush_l2(gpusw_ctx* c, int64_t bytes) {
 }
 
 }  // extern "C"
+#include "server.cuh"

@@ -145,6 +145,69 @@ int gpusw_measure_dpx_rate(gpusw_ctx *ctx, double *ops_per_s);
  * between timed steps of a benchmark). No reference counterpart (measurement only). */
 int gpusw_flush_l2(gpusw_ctx *ctx, int64_t bytes);
 
+/* ---------------------------------------------------------------------------------
+ * Serving: continuous batching over a resident reference set.
+ *
+ * A server keeps the reference set `rdb` of `ctx` resident and answers top-k requests.
+ * A scheduler thread admits pending requests in arrival order while a slot (an execution
+ * stream) and the device-memory budget allow, merges the admitted requests into one batch
+ * (up to max_batch_queries queries), and launches the batch asynchronously; batches on
+ * different slots overlap on the device. Each request's top-k equals what gpusw_topk
+ * returns for its queries alone. `ctx` must not be used for other calls while its server
+ * exists. No reference counterpart (the reference has no serving layer); this is the
+ * serving pattern of the scoring path.
+ * --------------------------------------------------------------------------------- */
+typedef struct gpusw_server gpusw_server;
+
+#define GPUSW_REQ_PENDING 0
+#define GPUSW_REQ_RUNNING 1
+#define GPUSW_REQ_DONE 2
+#define GPUSW_REQ_CANCELLED 3
+
+typedef struct gpusw_server_stats {
+  int64_t submitted, completed, cancelled, rejected;
+  int64_t pending, running;      /* requests waiting / on the device now */
+  int64_t batches;               /* launched batches */
+  double mean_batch_queries;
+  double p50_ms, p99_ms, mean_ms, max_ms;  /* submit -> done latency of completed requests */
+  double cells;                  /* DP cells of completed requests */
+  double wall_s;                 /* seconds since the first submit */
+  double gcups;                  /* cells / wall_s / 1e9 */
+  int64_t device_bytes;          /* device memory held by the server's slots */
+} gpusw_server_stats;
+
+/* Create a server over reference set `rdb` of `ctx` (scheme as set on ctx at this time).
+ * mem_budget bounds the device memory of in-flight batches (0: 4 GiB); max_slots (1-8)
+ * bounds concurrent batches; max_pending bounds queued requests (submit then returns
+ * GPUSW_ERR_QUEUE_FULL). */
+int gpusw_server_create(gpusw_ctx *ctx, int32_t rdb, int32_t k, int dtype, int64_t mem_budget,
+                        int32_t max_slots, int32_t max_batch_queries, int32_t max_pending,
+                        gpusw_server **out);
+
+/* Queue one request of nq encoded queries (codes/offsets as for gpusw_db_upload; copied,
+ * the caller may free them on return). *req_id receives its id. */
+int gpusw_server_submit(gpusw_server *srv, const uint8_t *codes, const int32_t *offsets,
+                        int32_t nq, int64_t *req_id);
+
+/* State of a request. When it is done, its (nq, min(k, n_refs)) top-k is copied into
+ * out_idx/out_score (may be NULL to discard) and the request is released; a cancelled
+ * request is released as well. Waits at most timeout_ms (0: no wait) for completion;
+ * GPUSW_ERR_NOT_FOUND for unknown or already released ids. */
+int gpusw_server_poll(gpusw_server *srv, int64_t req_id, int32_t timeout_ms, int32_t *state,
+                      int32_t *out_idx, int32_t *out_score);
+
+/* Cancel a request: a pending one is dropped at once, a running one has its results
+ * discarded when its batch finishes. */
+int gpusw_server_cancel(gpusw_server *srv, int64_t req_id);
+
+int gpusw_server_get_stats(gpusw_server *srv, gpusw_server_stats *out);
+
+/* Message of the last failed call on the server. */
+const char *gpusw_server_last_error(const gpusw_server *srv);
+
+/* Stop the scheduler (waiting at most for the in-flight batches) and free the server. */
+void gpusw_server_destroy(gpusw_server *srv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -103,6 +103,13 @@ class Group:
             self.dist.destroy_process_group()
 
 
+def aggregate(group, world: int, cells_per_rank: float, steps: int, step_ms: list) -> tuple:
+    """Whole-job GCUPS of `world` replicas: every rank scored `cells_per_rank` per step;
+    the job time is the slowest rank's summed device time. Returns (gcups, max_ms)."""
+    max_ms = group.max(float(sum(step_ms)))
+    return world * cells_per_rank * steps / (max_ms * 1e-3) / 1e9, max_ms
+
+
 def workload(name: str, nq=None, nr=None):
     from gpusw_b200 import workloads
 
@@ -383,8 +390,7 @@ def run_ours(args, rank, world, local):
     ctx.sync()
     group.barrier()
     clocks = sampler.stop()
-    total_ms = group.max(sum(times))
-    value = world * cells * args.steps / (total_ms * 1e-3) / 1e9
+    value, total_ms = aggregate(group, world, cells, args.steps, times)
     kern_gcups = cells * args.steps / (sum(score_ms) * 1e-3) / 1e9
     peak_gcups = dpx * 2.0 / OPS_PER_CELL_PAIR / 1e9
 

@@ -79,7 +79,9 @@ _SIGNATURES = {
     "gpusw_score_pairs": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
                            ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p],
                           ctypes.c_int),
-    "gpusw_set_options": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int64], ctypes.c_int),
+    "gpusw_set_options": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int], ctypes.c_int),
+    "gpusw_autotune": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_int32],
+                       ctypes.c_int),
     "gpusw_get_stats": ([ctypes.c_void_p, ctypes.POINTER(Stats)], ctypes.c_int),
     "gpusw_sync": ([ctypes.c_void_p], ctypes.c_int),
     "gpusw_measure_dpx_rate": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
@@ -181,8 +183,17 @@ class Context:
             int(sub.shape[0]), _ptr(sub)))
         self._scheme_key = key
 
-    def set_options(self, plain: bool = False, mem_budget: int = 0) -> None:
-        self._check(self.lib.gpusw_set_options(self.handle, int(bool(plain)), int(mem_budget)))
+    def set_options(self, plain: bool = False, mem_budget: int = 0, autotune: bool = True,
+                    graphs: bool = True) -> None:
+        flags = (0 if autotune else 1) | (0 if graphs else 2)
+        self._check(self.lib.gpusw_set_options(self.handle, int(bool(plain)), int(mem_budget), flags))
+
+    def autotune(self, width: int = 2) -> list[float]:
+        """(Re)tune the streaming kernel shapes for the current scheme; microseconds per
+        (reference row, column pass) of every compiled shape."""
+        out = (ctypes.c_double * 64)()
+        self._check(self.lib.gpusw_autotune(self.handle, int(width), out, 64))
+        return [out[i] for i in range(64) if out[i] > 0]
 
     # ------------------------------------------------------------------ sequence sets
     def upload(self, codes: np.ndarray, offsets: np.ndarray) -> int:

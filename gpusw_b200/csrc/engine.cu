@@ -186,6 +186,8 @@ struct gpusw_ctx {
   unsigned long long use_clock = 0;
   long long scheme_version = 0;
   int graphs = 1;              // replay cached plans as CUDA graphs
+  int autotune = 1;            // tune stream shapes on first use
+  std::vector<std::pair<std::pair<int, int>, std::vector<double>>> tune;  // (ns, P) -> us/row-pass
   gpusw_stats st{};
 };
 
@@ -431,6 +433,9 @@ void launch_overflow_rescore(gpusw_ctx* c, Bufs& B, const Db& q, const Db& r, in
   launch_pairs(c, B, shape, 1, c->sch.mode == gsw::kModeLocal, pp, std::max(q.max_len, r.max_len), true);
 }
 
+void run_cross(gpusw_ctx* c, Bufs& B, const Db& q, const Db& r, const int32_t* qlist, int nq, int P,
+               int* out, long long out_ld);
+
 // Stream buffer of a reference set in sorted (batched) or input (plain) order.
 const Db::Stream& get_stream(gpusw_ctx* c, Db& r, bool plain) {
   const int pad = c->sch.ns;
@@ -543,7 +548,7 @@ double stream_cost(const Shape& s, int ncols) {
 // Batched form: the shape (and pass count) of least modelled cost for this column length.
 // Plain form: one shape per call -- the smallest single-pass shape that covers the call's
 // longest query, or the widest shape in several passes when none covers it.
-int pick_stream_shape(int ncols, int ns, bool plain) {
+int pick_stream_shape(int ncols, int ns, bool plain, const std::vector<double>* tuned = nullptr) {
   int best = -1;
   double bc = 0;
   if (plain) {
@@ -558,13 +563,109 @@ int pick_stream_shape(int ncols, int ns, bool plain) {
   }
   for (int i = 0; i < kNumStream; ++i) {
     if (profile_bytes(kStreamShapes[i], ns) > kSmemCap) continue;
-    const double cst = stream_cost(kStreamShapes[i], ncols);
+    const double cst = tuned && (*tuned)[i] > 0
+                           ? (double)((std::max(ncols, 1) + kStreamShapes[i].cap() - 1) /
+                                      kStreamShapes[i].cap()) * (*tuned)[i]
+                           : stream_cost(kStreamShapes[i], ncols);
     if (best < 0 || cst < bc) {
       best = i;
       bc = cst;
     }
   }
   return best;
+}
+
+const std::vector<double>* find_tune(gpusw_ctx* c, int P) {
+  for (auto& kv : c->tune)
+    if (kv.first == std::make_pair(c->sch.ns, P)) return &kv.second;
+  return nullptr;
+}
+
+// Time every stream shape on synthetic full-width columns (256 queries of exactly G*W
+// residues) against 4,096 synthetic references of 300 residues -- thousands of work items
+// for every shape, so the GPU is full and the time measures throughput, not parallelism;
+// microseconds of device time per (reference row, column pass) of one column pair. Needs
+// no caller data; runs on the context's stream (about a second in all).
+std::vector<double> run_autotune(gpusw_ctx* c, int P) {
+  const HostScheme& h = c->sch;
+  std::vector<double> us(kNumStream, 0.0);
+  if (h.mode != gsw::kModeLocal || h.ns > 126) return us;
+  const int nr = 4096, mr = 300, nq = 256;
+  uint64_t rs = 0x9E3779B97F4A7C15ull;
+  auto rnd = [&]() { rs ^= rs << 13; rs ^= rs >> 7; rs ^= rs << 17; return rs; };
+  const int ncode = std::max(1, h.ns - 1);
+  std::vector<uint8_t> rc((size_t)nr * mr);
+  for (auto& v : rc) v = (uint8_t)(rnd() % ncode);
+  std::vector<int32_t> ro(nr + 1);
+  for (int i = 0; i <= nr; ++i) ro[i] = i * mr;
+  int32_t rdb = 0;
+  if (gpusw_db_upload(c, rc.data(), ro.data(), nr, &rdb) != GPUSW_OK) fail(GPUSW_ERR_CUDA, c->err);
+  Db& r = get_db(c, rdb);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int saved_plain = c->plain;
+  c->plain = 0;
+  Bufs T;  // private buffers: never disturbs a call's shared set
+  T.set_held(&c->held);
+  try {
+    for (int sh = 0; sh < kNumStream; ++sh) {
+      const Shape S = kStreamShapes[sh];
+      if (profile_bytes(S, h.ns) > kSmemCap) continue;
+      std::vector<uint8_t> qc((size_t)nq * S.cap());
+      for (auto& v : qc) v = (uint8_t)(rnd() % ncode);
+      std::vector<int32_t> qo(nq + 1);
+      for (int i = 0; i <= nq; ++i) qo[i] = i * S.cap();
+      int32_t qdb = 0;
+      if (gpusw_db_upload(c, qc.data(), qo.data(), nq, &qdb) != GPUSW_OK) fail(GPUSW_ERR_CUDA, c->err);
+      Db& q = get_db(c, qdb);
+      // force this shape: a one-shape table
+      std::vector<double> only(kNumStream, 1e30);
+      only[sh] = 1.0;
+      std::pair<std::pair<int, int>, std::vector<double>> entry({h.ns, P}, only);
+      c->tune.push_back(entry);
+      std::vector<int32_t> ql(nq);
+      std::iota(ql.begin(), ql.end(), 0);
+      int* d_out = T.out.as<int>((size_t)nq * nr);
+      double best = 1e30;
+      for (int rep = 0; rep < 2; ++rep) {
+        T.reset_marks();
+        CK(cudaEventRecord(e0, c->stream));
+        run_cross(c, T, q, r, ql.data(), nq, P, d_out, nr);
+        CK(cudaEventRecord(e1, c->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (rep > 0) best = std::min(best, (double)ms);
+      }
+      c->tune.pop_back();
+      us[sh] = best * 1e3 / ((double)((nq + P - 1) / P) * nr);
+      gpusw_db_free(c, qdb);
+    }
+  } catch (...) {
+    c->plain = saved_plain;
+    cudaStreamSynchronize(c->stream);
+    T.release();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    gpusw_db_free(c, rdb);
+    throw;
+  }
+  c->plain = saved_plain;
+  CK(cudaStreamSynchronize(c->stream));
+  T.release();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  gpusw_db_free(c, rdb);
+  return us;
+}
+
+// Tune on first use (at the entry of a call, before it takes any buffer).
+void ensure_tuned(gpusw_ctx* c, int P) {
+  if (!c->autotune || c->plain || c->sch.mode != gsw::kModeLocal || c->sch.ns > 126) return;
+  if (find_tune(c, P)) return;
+  std::vector<double> us = run_autotune(c, P);
+  c->tune.emplace_back(std::make_pair(c->sch.ns, P), us);
 }
 
 // Local-mode cross product through the streaming kernel (any column length).
@@ -589,8 +690,9 @@ void run_cross_stream(gpusw_ctx* c, Bufs& B, const Db& q, Db& r, const int32_t* 
   }
   std::vector<std::vector<int>> bins(kNumStream);
   const int call_max = npairs ? *std::max_element(pair_cols.begin(), pair_cols.end()) : 0;
+  const std::vector<double>* tuned = c->plain ? nullptr : find_tune(c, P);
   for (int i = 0; i < npairs; ++i) {
-    const int sh = pick_stream_shape(c->plain ? call_max : pair_cols[i], h.ns, c->plain != 0);
+    const int sh = pick_stream_shape(c->plain ? call_max : pair_cols[i], h.ns, c->plain != 0, tuned);
     if (sh < 0) fail(GPUSW_ERR_SCHEME, "substitution table too large for the profile");
     bins[sh].push_back(i);
   }
@@ -1192,6 +1294,7 @@ int gpusw_score_cross(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qli
     begin_call(c);
     const long long total = (long long)nq * r.n;
     const int P = choose_width(c, dtype, max_n, r.max_len);
+    if (total > 0) ensure_tuned(c, P);
     const std::vector<long long> key = {0, qdb, rdb, c->scheme_version, P, c->plain, nq, 0,
                                         (long long)fnv1a(qlist, (size_t)nq * 4)};
     auto body = [&](Bufs& B) {
@@ -1245,6 +1348,7 @@ int gpusw_topk(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qlist, int
     begin_call(c);
     if (nq > 0 && kk > 0) {
       int P = choose_width(c, dtype, max_n, r.max_len);
+      ensure_tuned(c, P);
       const long long row_bytes = (long long)r.n * 4;
       int qb = (int)std::max(1ll, std::min<long long>(nq, c->mem_budget / std::max(1ll, row_bytes)));
       if (c->plain) qb = std::min(qb, 16);
@@ -1436,11 +1540,29 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
   });
 }
 
-int gpusw_set_options(gpusw_ctx* c, int plain, int64_t mem_budget) {
+int gpusw_set_options(gpusw_ctx* c, int plain, int64_t mem_budget, int flags) {
   return guarded(c, [&] {
     if (mem_budget < 0) fail(GPUSW_ERR_INVALID, "negative memory budget");
     c->plain = plain ? 1 : 0;
     c->mem_budget = mem_budget ? mem_budget : (4ll << 30);
+    c->autotune = (flags & GPUSW_OPT_NO_AUTOTUNE) ? 0 : 1;
+    c->graphs = (flags & GPUSW_OPT_NO_GRAPHS) ? 0 : 1;
+  });
+}
+
+int gpusw_autotune(gpusw_ctx* c, int width, double* us_per_row_pass, int32_t n) {
+  return guarded(c, [&] {
+    if (!c->has_scheme) fail(GPUSW_ERR_SCHEME, "no scheme set");
+    if (width != 1 && width != 2) fail(GPUSW_ERR_INVALID, "width must be 1 (int32) or 2 (int16x2)");
+    set_device(c);
+    std::vector<double> us = run_autotune(c, width);
+    c->tune.erase(std::remove_if(c->tune.begin(), c->tune.end(),
+                                 [&](const auto& kv) { return kv.first == std::make_pair(c->sch.ns, width); }),
+                  c->tune.end());
+    c->tune.emplace_back(std::make_pair(c->sch.ns, width), us);
+    c->plans.clear();  // plans were binned with the previous costs
+    if (us_per_row_pass)
+      for (int i = 0; i < std::min<int>(n, (int)us.size()); ++i) us_per_row_pass[i] = us[i];
   });
 }
 

@@ -307,6 +307,8 @@ int gpusw_server_create(gpusw_ctx* ctx, int32_t rdb, int32_t k, int dtype, int64
     srv->max_pending = max_pending;
     set_device(ctx);
     if (ctx->sch.mode == gsw::kModeLocal && ctx->sch.ns <= 126) get_stream(ctx, r, false);
+    ensure_tuned(ctx, 2);
+    ensure_tuned(ctx, 1);
     CK(cudaStreamSynchronize(ctx->stream));
     for (int i = 0; i < max_slots; ++i) {
       auto sl = std::make_unique<Slot>();
@@ -316,6 +318,7 @@ int gpusw_server_create(gpusw_ctx* ctx, int32_t rdb, int32_t k, int dtype, int64
       src = gpusw_set_scheme(sl->ctx, h.mode, h.go, h.ge, h.free_q, h.free_r, h.ns, h.sub.data());
       if (src != GPUSW_OK) fail(src, gpusw_last_error(sl->ctx));
       for (DevBuf* b : {&sl->words, &sl->woff, &sl->len, &sl->perm, &sl->ident}) b->held = &sl->ctx->held;
+      sl->ctx->tune = ctx->tune;
       CK(cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming));
       srv->slots.push_back(std::move(sl));
     }

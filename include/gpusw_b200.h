@@ -126,8 +126,22 @@ int gpusw_score_pairs(gpusw_ctx *ctx, int32_t qdb, int32_t rdb, const int32_t *q
 /* Engine options. plain != 0 selects the one-batch-per-call form (queries in input order,
  * one kernel shape per batch, no length binning, no graph) used as the comparison point
  * of the batched form. mem_budget bounds the score blocks of gpusw_topk (bytes, 0 keeps the
- * default of 4 GiB). */
-int gpusw_set_options(gpusw_ctx *ctx, int plain, int64_t mem_budget);
+ * default of 4 GiB). flags: GPUSW_OPT_NO_AUTOTUNE keeps the modelled kernel-shape costs,
+ * GPUSW_OPT_NO_GRAPHS runs every call eagerly instead of replaying cached CUDA graphs. */
+#define GPUSW_OPT_NO_AUTOTUNE 1
+#define GPUSW_OPT_NO_GRAPHS 2
+int gpusw_set_options(gpusw_ctx *ctx, int plain, int64_t mem_budget, int flags);
+
+/* Autotune the streaming cross-product kernel for the current scheme: every compiled
+ * shape (team size G x columns per lane W) is timed once on synthetic full-width
+ * columns (256 queries) against 4,096 synthetic 300-residue references, enough work
+ * items to fill the GPU for every shape; the measured device time per (column pair,
+ * reference, column pass) replaces the modelled cost when the planner bins queries by
+ * length, so the bin edges are the crossover points of the measured costs. Tables are
+ * kept per (alphabet size, int width) in the context; calls run it on first use unless
+ * gpusw_set_options disabled it. us_per_row_pass (may be NULL) receives up to n entries
+ * (microseconds, one per shape). No reference counterpart. */
+int gpusw_autotune(gpusw_ctx *ctx, int width, double *us_per_row_pass, int32_t n);
 
 /* Counters (see gpusw_stats). Replaces src/gpusw/aligner.py:212 (Aligner.gcups): GCUPS =
  * last_cells / last_kernel_ms / 1e6. */

@@ -109,3 +109,20 @@ def test_overflow_rescore_through_graph_replay():
         tk = al.top_k(k=3)
         idx, sc = oracle.topk_stable(want, 3)
         assert np.array_equal(tk.topk_idx, idx) and np.array_equal(tk.topk_scores, sc)
+
+
+def test_autotune_table_and_results_unchanged():
+    qs, rs = _sets(6, nq=30, nr=200, alpha="ARNDCQEGHILKMFPSTWYV", lo=10, hi=1500)
+    sch = schemes.BLOSUM62
+    ctx = _native.context(0)
+    al = Aligner(sch).index(rs).set_queries(qs)
+    ctx.set_scheme(sch)
+    table = ctx.autotune(2)
+    assert len(table) >= 10 and all(t > 0 for t in table)
+    want = oracle.score_cross(funnel(qs, sch), funnel(rs, sch), sch)
+    assert np.array_equal(al.score_cross().astype(np.int64), want)
+    try:
+        ctx.set_options(autotune=False, graphs=False)
+        assert np.array_equal(al.score_cross().astype(np.int64), want)
+    finally:
+        ctx.set_options()

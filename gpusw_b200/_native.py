@@ -86,6 +86,10 @@ _SIGNATURES = {
     "gpusw_sync": ([ctypes.c_void_p], ctypes.c_int),
     "gpusw_measure_dpx_rate": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "gpusw_flush_l2": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+    "gpusw_score_pairs_noalloc": ([_VP, _VP, _I32, _VP, _VP, _I32, _VP, _VP, _I32, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_int, _VP, _I32, _VP, _VP, ctypes.c_char_p, _I32],
+                                  ctypes.c_int),
     "gpusw_server_create": ([_VP, _I32, _I32, ctypes.c_int, _I64, _I32, _I32, _I32,
                              ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "gpusw_server_submit": ([_VP, _VP, _VP, _I32, ctypes.POINTER(_I64)], ctypes.c_int),

@@ -114,6 +114,29 @@ struct Packed {
   }
 };
 
+// A sequence set as the reference package encodes it (one code byte per residue,
+// int32 offsets of n + 1 entries), read in place from caller-owned device memory.
+struct ByteSeqs {
+  const uint8_t* codes;
+  const int* off;
+  int n;
+  __device__ __forceinline__ int length(int s) const { return off[s + 1] - off[s]; }
+  __device__ __forceinline__ int code(int s, int c) const { return (int)__ldg(codes + off[s] + c); }
+};
+
+// Lane 0's code feed for a byte-coded row: the team_pass call passes the row's first
+// byte through its word-pointer parameter; one byte per step, the pad code past the end.
+struct RowFeed8 {
+  const uint8_t* p;
+  int m, pad;
+  __device__ __forceinline__ void init(const uint32_t* w, int, int, int m_, int pad_) {
+    p = reinterpret_cast<const uint8_t*>(w);
+    m = m_;
+    pad = pad_;
+  }
+  __device__ __forceinline__ int next(int t) const { return t < m ? (int)__ldg(p + t) : pad; }
+};
+
 // Lane 0's code feed for one row sequence: one packed word per `per` steps.
 struct RowFeed {
   const uint32_t* ptr;
@@ -167,7 +190,7 @@ struct Acc {
 // the last pass, so the end-column maximum costs one op per step instead of one per cell,
 // and the end row needs no column mask (the dummy columns hold 0, which the result takes
 // as a floor anyway).
-template <int G, int W, int P, bool LOCAL, bool PAIRS, bool LEFTPAD = false>
+template <int G, int W, int P, bool LOCAL, bool PAIRS, bool LEFTPAD = false, class Feed = RowFeed>
 __device__ __forceinline__ void team_pass(const SchemeDev& S, const uint4* __restrict__ prof,
                                           int pstride, const uint32_t* row_w0,
                                           const uint32_t* row_w1, int row_bits, int row_per,
@@ -203,7 +226,7 @@ __device__ __forceinline__ void team_pass(const SchemeDev& S, const uint4* __res
   uint32_t xb = Ops::splat((ladder_col0 ? S.go : 0) + S.go);
   const uint32_t xb_step = ladder_col0 ? GE : 0u;
 
-  RowFeed f0, f1;
+  Feed f0, f1;
   f0.init(row_w0, row_bits, row_per, m0, S.pad_code);
   if (PAIRS) f1.init(row_w1, row_bits, row_per, m1, S.pad_code);
 
@@ -351,9 +374,9 @@ __device__ __forceinline__ void team_pass(const SchemeDev& S, const uint4* __res
 // with other lanes is needed. `sub` may point to shared memory. pad0/pad1 shift the
 // halves' columns right (LEFTPAD); positions left of a sequence score 0, positions past
 // its end score s_pad.
-template <int G, int W, int P>
+template <int G, int W, int P, class Seqs = Packed>
 __device__ __forceinline__ void build_profile_lane(const SchemeDev& S, const int* sub,
-                                                   const Packed& cols, int c0, int n0, int pad0,
+                                                   const Seqs& cols, int c0, int n0, int pad0,
                                                    int c1, int n1, int pad1, int col0,
                                                    uint4* prof, int pstride, int lane) {
   const int pad_s = S.s_pad - S.go, zero_s = -S.go;

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 #include <string>
@@ -1615,4 +1616,177 @@ int gpusw_flush_l2(gpusw_ctx* c, int64_t bytes) {
 }
 
 }  // extern "C"
+
+// ==================================================================== no-allocation entry
+// gpusw_score_pairs_noalloc: explicit pairs from caller-owned device memory, with every
+// byte of scratch in the file-scope array below instead of memory the library allocates.
+// Layout: [0, 256) control (work counter, error word, failing pair); [256, 256 + 16 KiB)
+// substitution table (ns <= 64); the rest holds multi-pass boundary strips.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 32u << 20;  // 32 MiB on every device that loads us
+constexpr size_t kNoAllocSubOff = 256;
+constexpr size_t kNoAllocStripOff = kNoAllocSubOff + 64 * 64 * 4;
+constexpr int kNoAllocMaxDevices = 64;
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+void noalloc_msg(char* buf, int len, const char* msg) {
+  if (buf && len > 0) snprintf(buf, (size_t)len, "%s", msg);
+}
+
+template <bool L, bool LP>
+cudaError_t noalloc_launch(const gsw::NoAllocParams& prm, int grid, int teams, size_t smem,
+                           cudaStream_t st) {
+  auto k = gsw::pairs_noalloc_kernel<16, 16, L, LP>;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(kSmemCap));
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  k<<<grid, 16 * teams, smem, st>>>(prm);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" int gpusw_score_pairs_noalloc(const uint8_t* q_codes, const int32_t* q_offsets,
+                                         int32_t nq, const uint8_t* r_codes,
+                                         const int32_t* r_offsets, int32_t nr, const int32_t* qi,
+                                         const int32_t* rj, int32_t n, int mode, int gap_open,
+                                         int gap_extend, int free_q, int free_r, int ns,
+                                         const int32_t* sub, int32_t max_len, int32_t* out,
+                                         void* stream, char* errbuf, int32_t errlen) {
+  if (n < 0 || nq < 0 || nr < 0 || max_len < 1) {
+    noalloc_msg(errbuf, errlen, "negative count or max_len < 1");
+    return GPUSW_ERR_INVALID;
+  }
+  if (n == 0) return GPUSW_OK;
+  if (!q_codes || !q_offsets || !r_codes || !r_offsets || !qi || !rj || !out || !sub) {
+    noalloc_msg(errbuf, errlen, "null pointer argument");
+    return GPUSW_ERR_INVALID;
+  }
+  if (mode < 0 || mode > 2 || gap_open > 0 || gap_extend > 0 || gap_open < -(1 << 24) ||
+      gap_extend < -(1 << 24)) {
+    noalloc_msg(errbuf, errlen, "bad mode or gap costs");
+    return GPUSW_ERR_SCHEME;
+  }
+  if (ns < 2 || ns > 64) {
+    noalloc_msg(errbuf, errlen, "substitution table side must be in [2, 64] for this entry point");
+    return GPUSW_ERR_SCHEME;
+  }
+  HostScheme h;  // scalars only: no table copy, nothing allocated
+  h.mode = mode;
+  h.go = gap_open;
+  h.ge = gap_extend;
+  h.free_q = free_q ? 1 : 0;
+  h.free_r = free_r ? 1 : 0;
+  h.ns = ns;
+  h.max_sub = h.min_sub = sub[0];
+  for (int i = 0; i < ns * ns; ++i) {
+    h.max_sub = std::max(h.max_sub, (int)sub[i]);
+    h.min_sub = std::min(h.min_sub, (int)sub[i]);
+  }
+  if (h.max_sub > (1 << 24) || h.min_sub < -(1 << 24)) {
+    noalloc_msg(errbuf, errlen, "substitution scores beyond +/-2^24");
+    return GPUSW_ERR_SCHEME;
+  }
+  if (!width_ok(h, 1, max_len, max_len)) {
+    noalloc_msg(errbuf, errlen, "scores of this scheme and max_len do not fit in int32");
+    return GPUSW_ERR_OVERFLOW;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+    cudaGetLastError();
+    noalloc_msg(errbuf, errlen, "no usable current CUDA device");
+    return GPUSW_ERR_NO_GPU;
+  }
+  unsigned char* base = nullptr;
+  {
+    // once per device, with that device current: the device address of the scratch array
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* ptr = nullptr;
+      if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) {
+        cudaGetLastError();
+        noalloc_msg(errbuf, errlen, "cudaGetSymbolAddress of the scratch array failed");
+        return GPUSW_ERR_CUDA;
+      }
+      g_noalloc_ptr[dev] = ptr;
+    }
+    base = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    noalloc_msg(errbuf, errlen, "cudaDeviceGetAttribute failed");
+    return GPUSW_ERR_CUDA;
+  }
+  const Shape shape{16, 16};
+  const size_t prof = profile_bytes(shape, ns);
+  const int teams = (int)std::max<size_t>(1, std::min<size_t>(16, kSmemCap / prof));
+  const size_t smem = prof * teams;
+  // boundary strips only when a column sequence can be longer than one pass
+  const bool multipass = max_len > shape.cap();
+  const size_t strip_bytes = kNoAllocScratchBytes - kNoAllocStripOff;
+  long long grid = (long long)sms * 2;
+  if (multipass) {
+    const long long fit = (long long)(strip_bytes / ((size_t)teams * (size_t)max_len * sizeof(uint2)));
+    if (fit < 1) {
+      char msg[160];
+      snprintf(msg, sizeof msg, "max_len %d exceeds the %zu residues the no-allocation scratch holds",
+               max_len, strip_bytes / ((size_t)teams * sizeof(uint2)));
+      noalloc_msg(errbuf, errlen, msg);
+      return GPUSW_ERR_MEMORY;
+    }
+    grid = std::min(grid, fit);
+  }
+  grid = std::max(1ll, std::min<long long>(grid, ((long long)n + teams - 1) / teams));
+  gsw::NoAllocParams prm{};
+  prm.S = make_scheme(h, 1);
+  prm.sub = reinterpret_cast<const int*>(base + kNoAllocSubOff);
+  prm.cols = gsw::ByteSeqs{q_codes, q_offsets, nq};
+  prm.rows = gsw::ByteSeqs{r_codes, r_offsets, nr};
+  prm.qi = qi;
+  prm.rj = rj;
+  prm.n = n;
+  prm.out = out;
+  prm.queue = reinterpret_cast<unsigned long long*>(base);
+  prm.err = reinterpret_cast<int*>(base + 8);
+  prm.bnd = multipass ? reinterpret_cast<uint2*>(base + kNoAllocStripOff) : nullptr;
+  prm.bnd_cap = multipass ? max_len : 0;
+  prm.max_len = max_len;
+  // every call shares the array: clear the counter and error word, refresh the table
+  cudaError_t e = cudaMemsetAsync(base, 0, 16, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(base + kNoAllocSubOff, sub, (size_t)ns * ns * sizeof(int32_t),
+                        cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    const bool local = mode == gsw::kModeLocal, lp = mode == gsw::kModeSemi && free_q && free_r;
+    e = local ? noalloc_launch<true, false>(prm, (int)grid, teams, smem, st)
+              : lp ? noalloc_launch<false, true>(prm, (int)grid, teams, smem, st)
+                   : noalloc_launch<false, false>(prm, (int)grid, teams, smem, st);
+  }
+  int herr[2] = {0, 0};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(herr, base + 8, sizeof herr, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    noalloc_msg(errbuf, errlen, cudaGetErrorString(e));
+    return GPUSW_ERR_CUDA;
+  }
+  if (herr[0] != 0) {
+    char msg[128];
+    snprintf(msg, sizeof msg, herr[0] == 1 ? "pair index out of range at position %d"
+                                           : "row longer than max_len at pair %d", herr[1]);
+    noalloc_msg(errbuf, errlen, msg);
+    return GPUSW_ERR_INVALID;
+  }
+  return GPUSW_OK;
+}
+
 #include "server.cuh"

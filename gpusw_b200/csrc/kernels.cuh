@@ -513,4 +513,87 @@ __global__ void build_stream_kernel(const Packed rows, const int* __restrict__ o
   for (int c = ln; c < m; c += 32) o[c] = (int8_t)(rows.code(r, c) | (c == m - 1 ? 0x80 : 0));
 }
 
+// -------------------------------------------------------------------------------------
+// Pairs scored from caller-owned device memory with no allocation by the library: the
+// reference package's byte codes and int32 offsets are read in place, scoring is int32
+// (one alignment per lane, so no int16 overflow list is needed), and the work counter,
+// the error word and the boundary strips live in a scratch area whose address the host
+// passes in. Indices and lengths are checked here: a bad pair is recorded in the error
+// word and skipped, its output left untouched.
+struct NoAllocParams {
+  SchemeDev S;
+  const int* sub;              // ns x ns substitution table in the scratch area
+  ByteSeqs cols, rows;
+  const int* qi;
+  const int* rj;
+  int n;
+  int* out;
+  unsigned long long* queue;   // scratch: work counter (zeroed by the host per call)
+  int* err;                    // scratch: [0] = 1 bad index, 2 row longer than a strip; [1] = pair
+  uint2* bnd;                  // scratch: boundary strips, one per team
+  int bnd_cap;                 // rows per strip (0: single-pass only)
+  int max_len;                 // the caller's bound on every sequence length
+};
+
+template <int G, int W, bool LOCAL, bool LEFTPAD>
+__global__ void __launch_bounds__(256) pairs_noalloc_kernel(const NoAllocParams p) {
+  extern __shared__ uint4 smem_prof[];
+  __shared__ int s_sub[kSubSmemMax * kSubSmemMax];
+  constexpr int SLOTS = G * W / 4;
+  const int pstride = (SLOTS + 7) & ~7;
+  const int team = threadIdx.x / G, lane = threadIdx.x % G, nteams = blockDim.x / G;
+  const unsigned wmask = (G == 32) ? 0xFFFFFFFFu
+                                   : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
+  const int ns = p.S.ns;
+  for (int i = threadIdx.x; i < ns * ns; i += blockDim.x) s_sub[i] = p.sub[i];
+  __syncthreads();
+  uint4* prof = smem_prof + (size_t)team * (ns + 1) * pstride;
+  uint2* bnd = p.bnd ? p.bnd + ((size_t)blockIdx.x * nteams + team) * p.bnd_cap : nullptr;
+  for (;;) {
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(p.queue, 1ull);
+    t = __shfl_sync(wmask, t, 0, G);
+    if ((long long)t >= p.n) break;
+    const int k = (int)t;
+    const int q = p.qi[k], r = p.rj[k];
+    if (q < 0 || q >= p.cols.n || r < 0 || r >= p.rows.n) {
+      if (lane == 0 && atomicCAS(p.err, 0, 1) == 0) p.err[1] = k;
+      continue;
+    }
+    const int n0 = p.cols.length(q), m0 = p.rows.length(r);
+    if (n0 > p.max_len || m0 > p.max_len) {
+      if (lane == 0 && atomicCAS(p.err, 0, 2) == 0) p.err[1] = k;
+      continue;
+    }
+    Acc acc = init_acc<1>(p.S);
+    if (n0 > 0 && m0 > 0) {
+      const int npass = (n0 + G * W - 1) / (G * W);
+      if (npass > 1 && (bnd == nullptr || m0 > p.bnd_cap)) {
+        if (lane == 0 && atomicCAS(p.err, 0, 2) == 0) p.err[1] = k;
+        continue;
+      }
+      const int span = npass * G * W;
+      const int pad0 = LEFTPAD ? span - n0 : 0;
+      const uint32_t* w0 = reinterpret_cast<const uint32_t*>(p.rows.codes + p.rows.off[r]);
+      for (int ps = 0; ps < npass; ++ps) {
+        build_profile_lane<G, W, 1, ByteSeqs>(p.S, s_sub, p.cols, q, n0, pad0, -1, 0, 0,
+                                              ps * G * W, prof, pstride, lane);
+        team_pass<G, W, 1, LOCAL, true, LEFTPAD, RowFeed8>(
+            p.S, prof, pstride, w0, w0, 0, 0, m0, m0, LEFTPAD ? span : n0, LEFTPAD ? span : 0,
+            ps * G * W, bnd, ps > 0, ps + 1 < npass, lane, wmask, acc, ps + 1 == npass);
+        __syncwarp(wmask);
+      }
+      acc = reduce_acc<G, 1>(p.S, acc, wmask);
+    }
+    if (lane == 0) {
+      bool ovf = false;
+      int score;
+      if (n0 == 0 || m0 == 0) score = empty_score(p.S, n0, m0);
+      else if (LEFTPAD) score = finish_score_leftpad<1>(p.S, acc, 0, &ovf);
+      else score = finish_score<1>(p.S, acc, 0, &ovf);
+      p.out[k] = score;
+    }
+  }
+}
+
 }  // namespace gsw

@@ -159,6 +159,36 @@ int gpusw_measure_dpx_rate(gpusw_ctx *ctx, double *ops_per_s);
  * between timed steps of a benchmark). No reference counterpart (measurement only). */
 int gpusw_flush_l2(gpusw_ctx *ctx, int64_t bytes);
 
+/* Explicit pairs scored without any allocation by the library, for callers that own all
+ * device memory and cannot let a library call cudaMalloc: code running inside a framework's
+ * caching allocator or a fixed arena sized at start-up, plugin hosts that forbid allocation
+ * in their callbacks, or latency-bound loops that cannot pay the device-wide
+ * synchronisation a cudaFree implies. No counterpart in the reference (which allocates
+ * through CuPy on every call).
+ *
+ * Inputs and output are the caller's device memory, in the reference's own encoding: code
+ * bytes with int32 offsets (n_seq + 1) for the queries and the references, int32 pair
+ * indices qi/rj[n], int32 out[n] (out[i] = score of query qi[i] vs reference rj[i]). The
+ * substitution table `sub` (ns x ns int32, row = reference code) is a host array.
+ * max_len must bound every sequence length. Scores are computed in int32 and equal
+ * gpusw_score_pairs. The kernel's scratch (work counter, error word, table, multi-pass
+ * boundary strips) lives in a 32 MiB file-scope device array that every GPU loading this
+ * library holds until exit; sizes beyond it are rejected (GPUSW_ERR_MEMORY): ns <= 64, and
+ * with max_len above 256 the strips need max_len x 8 bytes per team (about 260,000
+ * residues at most). The first call on a device looks up the array's device address with
+ * that device current; make that first call before any stream capture. Every call shares
+ * the array and resets its counter and error word; calls that overlap on the GPU (on
+ * different streams or threads) race on it and must be serialised by the caller. Runs on
+ * `stream` (a cudaStream_t, NULL for the legacy default stream) and returns after the
+ * stream is idle. Bad indices or lengths above max_len are found on the device, skipped
+ * and reported as GPUSW_ERR_INVALID. Messages go to errbuf (errlen bytes, may be NULL). */
+int gpusw_score_pairs_noalloc(const uint8_t *q_codes, const int32_t *q_offsets, int32_t nq,
+                              const uint8_t *r_codes, const int32_t *r_offsets, int32_t nr,
+                              const int32_t *qi, const int32_t *rj, int32_t n, int mode,
+                              int gap_open, int gap_extend, int free_q, int free_r, int ns,
+                              const int32_t *sub, int32_t max_len, int32_t *out, void *stream,
+                              char *errbuf, int32_t errlen);
+
 /* ---------------------------------------------------------------------------------
  * Serving: continuous batching over a resident reference set.
  *

@@ -86,6 +86,9 @@ _SIGNATURES = {
     "gpusw_sync": ([ctypes.c_void_p], ctypes.c_int),
     "gpusw_measure_dpx_rate": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "gpusw_flush_l2": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+    "gpusw_get_tune": ([_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _I32], ctypes.c_int),
+    "gpusw_set_tune": ([_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _I32], ctypes.c_int),
+    "gpusw_device_name": ([ctypes.c_int, ctypes.c_char_p, _I32], ctypes.c_int),
     "gpusw_score_pairs_noalloc": ([_VP, _VP, _I32, _VP, _VP, _I32, _VP, _VP, _I32, ctypes.c_int,
                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_int, _VP, _I32, _VP, _VP, ctypes.c_char_p, _I32],
@@ -186,6 +189,49 @@ class Context:
             int(bool(scheme.free_end_gaps_query)), int(bool(scheme.free_end_gaps_ref)),
             int(sub.shape[0]), _ptr(sub)))
         self._scheme_key = key
+        if scheme.mode == "local":
+            self._load_tune(int(sub.shape[0]))
+
+    # ------------------------------------------------------------------ autotune cache
+    def _tune_path(self, ns: int, width: int) -> str | None:
+        root = os.environ.get("GPUSW_B200_TUNE_DIR",
+                              os.path.join(os.path.expanduser("~"), ".cache", "gpusw_b200"))
+        buf = ctypes.create_string_buffer(256)
+        if self.lib.gpusw_device_name(self.device, buf, 256) != OK:
+            return None
+        name = "".join(ch if ch.isalnum() else "_" for ch in buf.value.decode())
+        return os.path.join(root, f"tune-{name}-v{self.lib.gpusw_version()}-ns{ns}-w{width}.txt")
+
+    def _load_tune(self, ns: int) -> None:
+        """Install autotuner tables cached on disk by an earlier process (if any)."""
+        for width in (2, 1):
+            path = self._tune_path(ns, width)
+            if not path or not os.path.exists(path):
+                continue
+            have = self.lib.gpusw_get_tune(self.handle, width, None, 0)
+            if have > 0:
+                continue
+            try:
+                vals = [float(x) for x in open(path).read().split()]
+            except (OSError, ValueError):
+                continue
+            arr = (ctypes.c_double * len(vals))(*vals)
+            self.lib.gpusw_set_tune(self.handle, width, arr, len(vals))
+
+    def save_tune(self, ns: int) -> None:
+        """Write the context's autotuner tables for alphabet size `ns` to the disk cache."""
+        for width in (2, 1):
+            out = (ctypes.c_double * 64)()
+            got = self.lib.gpusw_get_tune(self.handle, width, out, 64)
+            path = self._tune_path(ns, width)
+            if got > 0 and path and not os.path.exists(path):
+                try:
+                    os.makedirs(os.path.dirname(path), exist_ok=True)
+                    with open(path + ".tmp", "w") as fh:
+                        fh.write(" ".join(repr(out[i]) for i in range(got)))
+                    os.replace(path + ".tmp", path)
+                except OSError:
+                    pass
 
     def set_options(self, plain: bool = False, mem_budget: int = 0, autotune: bool = True,
                     graphs: bool = True) -> None:

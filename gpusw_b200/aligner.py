@@ -129,6 +129,8 @@ class Aligner:
         return "auto"
 
     def _record(self, ctx: _native.Context, kernel: str) -> None:
+        if self.scheme.mode == "local":
+            ctx.save_tune(self.scheme.ns)
         st = ctx.stats()
         self._last_gcups = st.last_cells / (st.last_kernel_ms * 1e6) if st.last_kernel_ms > 0 else 0.0
         self._last_kernel = kernel

@@ -2,6 +2,7 @@
 // launch planner, the int16 -> int32 overflow rescoring and the C ABI of
 // include/gpusw_b200.h.
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cstdio>
 #include <cstring>
@@ -181,6 +182,8 @@ struct gpusw_ctx {
   int64_t held = 0;
   Bufs shared;
   DevBuf flush;
+  uint32_t* pinned = nullptr;  // host staging for set uploads (page-locked, grow-only)
+  size_t pinned_words = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
   Bufs* last_bufs = nullptr;  // the set whose stage marks the last call used
   std::vector<std::unique_ptr<Plan>> plans;
@@ -238,27 +241,35 @@ bool width_ok(const HostScheme& h, int P, long long max_n, long long max_m) {
 }
 
 // ------------------------------------------------------------------------- sequences
-void pack_host(const uint8_t* codes, const int32_t* offs, const Db& d, std::vector<uint32_t>& words) {
-  const int nthreads = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-  auto work = [&](int t) {
-    for (int s = t; s < d.n; s += nthreads) {
-      const uint8_t* src = codes + offs[s];
-      const int len = d.len[s];
-      uint32_t* dst = words.data() + d.woff[s];
-      for (int c = 0; c < len; c += d.per) {
-        uint32_t v = 0;
-        const int e_end = std::min(d.per, len - c);
-        for (int e = 0; e < e_end; ++e) v |= (uint32_t)src[c + e] << (e * d.bits);
-        dst[c / d.per] = v;
-      }
+int host_threads() { return (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency())); }
+
+// Run f(begin, end) over [0, n) split into contiguous ranges on the host's cores.
+template <class F>
+void parallel_ranges(long long n, F&& f) {
+  const int nt = n < (1 << 16) ? 1 : host_threads();
+  if (nt == 1) {
+    f(0ll, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; ++t) th.emplace_back([&, t] { f(n * t / nt, n * (t + 1) / nt); });
+  for (auto& x : th) x.join();
+}
+
+// Pack sequences [s0, s1) into words (each sequence's words including its alignment
+// padding, so the destination needs no prior zeroing).
+void pack_range(const uint8_t* codes, const int32_t* offs, const Db& d, uint32_t* words, int s0, int s1) {
+  for (int s = s0; s < s1; ++s) {
+    const uint8_t* src = codes + offs[s];
+    const int len = d.len[s];
+    uint32_t* dst = words + d.woff[s];
+    const long long nw = (s + 1 < d.n ? d.woff[s + 1] : d.woff[s] + (((len + d.per - 1) / d.per + 3) & ~3ll)) - d.woff[s];
+    int c = 0;
+    for (long long w = 0; w < nw; ++w) {
+      uint32_t v = 0;
+      for (int e = 0; e < d.per && c < len; ++e, ++c) v |= (uint32_t)src[c] << (e * d.bits);
+      dst[w] = v;
     }
-  };
-  if (d.n < 4096) {
-    for (int t = 0; t < nthreads; ++t) work(t);
-  } else {
-    std::vector<std::thread> th;
-    for (int t = 0; t < nthreads; ++t) th.emplace_back(work, t);
-    for (auto& x : th) x.join();
   }
 }
 
@@ -323,20 +334,35 @@ int pair_teams(const Shape& s, int ns) {
 }
 
 template <int G, int W, int P, bool L, bool LP>
-void launch_pairs_t(gpusw_ctx* c, Bufs& B, gsw::PairsParams prm, int teams, long long max_rows, bool multipass) {
+void launch_pairs_t(gpusw_ctx* c, Bufs& B, gsw::PairsParams prm, int /*teams_hint*/, long long max_rows, bool multipass) {
   auto k = gsw::pairs_kernel<G, W, P, L, LP>;
   const Shape s{G, W};
-  const size_t smem = profile_bytes(s, prm.S.ns) * teams;
+  const size_t sub_bytes = (size_t)gsw::pairs_sub_uint4(prm.S.ns) * 16;
+  const size_t prof = profile_bytes(s, prm.S.ns);
   static int configured_dev = -1;
   static size_t configured_smem = 0;
-  if (configured_dev != c->device || configured_smem < smem) {
-    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(smem, configured_smem)));
-    configured_smem = std::max(smem, configured_smem);
+  const size_t max_smem = 227 * 1024;
+  if (configured_dev != c->device) {
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+    configured_smem = max_smem;
     configured_dev = c->device;
   }
-  int bps = 1;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, G * teams, smem));
-  long long grid = (long long)c->sms * std::max(1, bps);
+  // teams per block: the count that keeps the most warps resident (ties: larger blocks)
+  int teams = 1, best_warps = -1, bps_best = 1;
+  for (int t = 1; t * G <= 256; t *= 2) {
+    const size_t smem = sub_bytes + prof * t;
+    if (smem > max_smem) break;
+    int bps = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, G * t, smem));
+    const int warps = bps * G * t / 32;
+    if (bps > 0 && warps >= best_warps) {
+      best_warps = warps;
+      teams = t;
+      bps_best = bps;
+    }
+  }
+  const size_t smem = sub_bytes + prof * teams;
+  long long grid = (long long)c->sms * std::max(1, bps_best);
   const long long team_items = prm.item_mode == 1 ? kOvfCap : prm.n_items;
   grid = std::max(1ll, std::min(grid, (team_items + teams - 1) / teams));
   if (multipass) {
@@ -1148,6 +1174,7 @@ void gpusw_ctx_destroy(gpusw_ctx* c) {
   c->plans.clear();
   c->shared.release();
   c->flush.release();
+  if (c->pinned) cudaFreeHost(c->pinned);
   if (c->sub_d) cudaFree(c->sub_d);
   for (cudaEvent_t e : {c->ev0, c->ev1, c->ev2, c->ev3})
     if (e) cudaEventDestroy(e);
@@ -1194,22 +1221,28 @@ int gpusw_db_upload(gpusw_ctx* c, const uint8_t* codes, const int32_t* offsets, 
   return guarded(c, [&] {
     if (!offsets || !out_db || n < 0) fail(GPUSW_ERR_INVALID, "null offsets/handle or negative count");
     if (offsets[0] < 0) fail(GPUSW_ERR_INVALID, "offsets must be non-negative");
-    for (int i = 0; i < n; ++i)
-      if (offsets[i + 1] < offsets[i]) fail(GPUSW_ERR_INVALID, "offsets must be non-decreasing");
-    const long long total = n ? (long long)offsets[n] - offsets[0] : 0;
-    if (total > 0 && !codes) fail(GPUSW_ERR_INVALID, "null codes");
     auto d = std::make_unique<Db>();
     d->n = n;
     d->len.resize(n);
-    int maxc = 0;
     for (int i = 0; i < n; ++i) {
+      if (offsets[i + 1] < offsets[i]) fail(GPUSW_ERR_INVALID, "offsets must be non-decreasing");
       d->len[i] = offsets[i + 1] - offsets[i];
       d->max_len = std::max(d->max_len, d->len[i]);
     }
-    if (n) {
-      const uint8_t* b = codes + offsets[0];
-      for (long long k = 0; k < total; ++k) maxc = std::max<int>(maxc, b[k]);
+    const long long total = n ? (long long)offsets[n] - offsets[0] : 0;
+    if (total > 0 && !codes) fail(GPUSW_ERR_INVALID, "null codes");
+    // largest code (threaded) -> bits per residue
+    std::vector<int> tmax(host_threads() + 1, 0);
+    {
+      const uint8_t* b0 = codes ? codes + offsets[0] : nullptr;
+      std::atomic<int> slot{0};
+      parallel_ranges(total, [&](long long lo, long long hi) {
+        int m = 0;
+        for (long long k = lo; k < hi; ++k) m = std::max<int>(m, b0[k]);
+        tmax[slot++] = m;
+      });
     }
+    const int maxc = *std::max_element(tmax.begin(), tmax.end());
     d->max_code = maxc;
     d->bits = maxc < 4 ? 2 : maxc < 16 ? 4 : maxc < 32 ? 5 : 8;
     d->per = d->bits == 5 ? 6 : 32 / d->bits;
@@ -1220,23 +1253,43 @@ int gpusw_db_upload(gpusw_ctx* c, const uint8_t* codes, const int32_t* offsets, 
       w += ((d->len[i] + d->per - 1) / d->per + 3) & ~3ll;
     }
     const long long nwords = w + 64;  // tail slack for read-ahead
-    std::vector<uint32_t> words((size_t)nwords, 0u);
+    set_device(c);
+    CK(cudaStreamSynchronize(c->stream));  // the staging buffer may still feed a copy
+    if ((size_t)nwords > c->pinned_words) {
+      if (c->pinned) cudaFreeHost(c->pinned);
+      c->pinned = nullptr;
+      c->pinned_words = 0;
+      CK(cudaMallocHost(&c->pinned, (size_t)nwords * 4));
+      c->pinned_words = (size_t)nwords;
+    }
     // offsets are relative to codes[0] in the ABI (like the reference's Encoded)
-    pack_host(codes, offsets, *d, words);
+    parallel_ranges(n, [&](long long lo, long long hi) { pack_range(codes, offsets, *d, c->pinned, (int)lo, (int)hi); });
+    std::fill(c->pinned + w, c->pinned + nwords, 0u);
+    // longest first, stable: two-pass radix sort on the complemented length
     d->perm_desc.resize(n);
-    std::iota(d->perm_desc.begin(), d->perm_desc.end(), 0);
-    std::stable_sort(d->perm_desc.begin(), d->perm_desc.end(),
-                     [&](int a, int b) { return d->len[a] > d->len[b]; });
+    {
+      std::vector<int> tmp(n);
+      std::iota(tmp.begin(), tmp.end(), 0);
+      std::vector<int> cnt(65537);
+      for (int pass = 0; pass < 2; ++pass) {
+        const int sh = pass * 16;
+        std::fill(cnt.begin(), cnt.end(), 0);
+        auto key = [&](int i) { return ((0x7FFFFFFFu - (uint32_t)d->len[i]) >> sh) & 0xFFFFu; };
+        for (int i = 0; i < n; ++i) cnt[key(tmp[i]) + 1]++;
+        for (int bk = 0; bk < 65536; ++bk) cnt[bk + 1] += cnt[bk];
+        for (int i = 0; i < n; ++i) d->perm_desc[cnt[key(tmp[i])]++] = tmp[i];
+        if (pass == 0) tmp.swap(d->perm_desc);
+      }
+    }
     std::vector<int> ident(n);
     std::iota(ident.begin(), ident.end(), 0);
-    set_device(c);
     CK(cudaMalloc(&d->words, nwords * sizeof(uint32_t)));
     CK(cudaMalloc(&d->woff_d, std::max(1, n) * sizeof(long long)));
     CK(cudaMalloc(&d->len_d, std::max(1, n) * sizeof(int)));
     CK(cudaMalloc(&d->perm_d, std::max(1, n) * sizeof(int)));
     CK(cudaMalloc(&d->ident_d, std::max(1, n) * sizeof(int)));
     d->bytes = nwords * 4 + (long long)std::max(1, n) * 20;
-    CK(cudaMemcpyAsync(d->words, words.data(), nwords * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d->words, c->pinned, nwords * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
     if (n) {
       CK(cudaMemcpyAsync(d->woff_d, d->woff.data(), n * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
       CK(cudaMemcpyAsync(d->len_d, d->len.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
@@ -1549,6 +1602,43 @@ int gpusw_set_options(gpusw_ctx* c, int plain, int64_t mem_budget, int flags) {
     c->autotune = (flags & GPUSW_OPT_NO_AUTOTUNE) ? 0 : 1;
     c->graphs = (flags & GPUSW_OPT_NO_GRAPHS) ? 0 : 1;
   });
+}
+
+int gpusw_get_tune(gpusw_ctx* c, int width, double* us, int32_t n) {
+  int copied = 0;
+  int rc = guarded(c, [&] {
+    if (!c->has_scheme) fail(GPUSW_ERR_SCHEME, "no scheme set");
+    const std::vector<double>* t = find_tune(c, width);
+    if (!t) return;
+    for (int i = 0; i < std::min<int>(n, (int)t->size()); ++i, ++copied)
+      if (us) us[i] = (*t)[i];
+  });
+  return rc == GPUSW_OK ? copied : -rc;
+}
+
+int gpusw_set_tune(gpusw_ctx* c, int width, const double* us, int32_t n) {
+  return guarded(c, [&] {
+    if (!c->has_scheme) fail(GPUSW_ERR_SCHEME, "no scheme set");
+    if (width != 1 && width != 2) fail(GPUSW_ERR_INVALID, "width must be 1 or 2");
+    if (!us || n != kNumStream) fail(GPUSW_ERR_INVALID, "table must have one entry per stream shape");
+    std::vector<double> t(us, us + n);
+    c->tune.erase(std::remove_if(c->tune.begin(), c->tune.end(),
+                                 [&](const auto& kv) { return kv.first == std::make_pair(c->sch.ns, width); }),
+                  c->tune.end());
+    c->tune.emplace_back(std::make_pair(c->sch.ns, width), t);
+    c->plans.clear();
+  });
+}
+
+int gpusw_device_name(int device, char* buf, int32_t len) {
+  if (!buf || len < 1) return GPUSW_ERR_INVALID;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+    cudaGetLastError();
+    return GPUSW_ERR_NO_GPU;
+  }
+  snprintf(buf, (size_t)len, "%s", prop.name);
+  return GPUSW_OK;
 }
 
 int gpusw_autotune(gpusw_ctx* c, int width, double* us_per_row_pass, int32_t n) {

@@ -229,23 +229,30 @@ __device__ __forceinline__ PairItem<P> decode_item(const PairsParams& p, long lo
 
 constexpr int kSubSmemMax = 64;  // substitution tables up to 64 x 64 are staged in shared memory
 
+// Dynamic shared memory of the pairs kernel: the substitution table (when ns <= 64, in
+// whole uint4) followed by one profile per team.
+__host__ __device__ __forceinline__ int pairs_sub_uint4(int ns) {
+  return ns <= kSubSmemMax ? (ns * ns + 3) / 4 : 0;
+}
+
 template <int G, int W, int P, bool LOCAL, bool LEFTPAD>
 __global__ void __launch_bounds__(256) pairs_kernel(const PairsParams p) {
   extern __shared__ uint4 smem_prof[];
-  __shared__ int s_sub[kSubSmemMax * kSubSmemMax];
   constexpr int SLOTS = G * W / 4;
   const int pstride = (SLOTS + 7) & ~7;
   const int team = threadIdx.x / G, lane = threadIdx.x % G, nteams = blockDim.x / G;
   const unsigned wmask = (G == 32) ? 0xFFFFFFFFu
                                    : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
   const int ns = p.S.ns;
+  const int sub_u4 = pairs_sub_uint4(ns);
   const int* sub = p.sub;
-  if (ns <= kSubSmemMax) {
+  if (sub_u4 > 0) {
+    int* s_sub = reinterpret_cast<int*>(smem_prof);
     for (int i = threadIdx.x; i < ns * ns; i += blockDim.x) s_sub[i] = p.sub[i];
     __syncthreads();
     sub = s_sub;
   }
-  uint4* prof = smem_prof + (size_t)team * (ns + 1) * pstride;
+  uint4* prof = smem_prof + sub_u4 + (size_t)team * (ns + 1) * pstride;
   uint2* bnd = p.bnd ? p.bnd + ((size_t)blockIdx.x * nteams + team) * p.bnd_cap : nullptr;
   long long n_items = p.n_items;
   if (p.item_mode == 1) {

@@ -143,6 +143,17 @@ int gpusw_set_options(gpusw_ctx *ctx, int plain, int64_t mem_budget, int flags);
  * (microseconds, one per shape). No reference counterpart. */
 int gpusw_autotune(gpusw_ctx *ctx, int width, double *us_per_row_pass, int32_t n);
 
+/* Read (get) or install (set) the autotuner table of the current scheme's alphabet size
+ * and `width` (1 = int32, 2 = int16x2), so that a caller can keep tables across processes.
+ * get returns the number of entries copied (0 when the context has no table yet, negative
+ * status on error); set replaces the table and drops cached plans. No reference
+ * counterpart. */
+int gpusw_get_tune(gpusw_ctx *ctx, int width, double *us_per_row_pass, int32_t n);
+int gpusw_set_tune(gpusw_ctx *ctx, int width, const double *us_per_row_pass, int32_t n);
+
+/* Name of CUDA device `device` (for cache keys); returns a status. */
+int gpusw_device_name(int device, char *buf, int32_t len);
+
 /* Counters (see gpusw_stats). Replaces src/gpusw/aligner.py:212 (Aligner.gcups): GCUPS =
  * last_cells / last_kernel_ms / 1e6. */
 int gpusw_get_stats(gpusw_ctx *ctx, gpusw_stats *out);

@@ -86,6 +86,7 @@ _SIGNATURES = {
     "gpusw_sync": ([ctypes.c_void_p], ctypes.c_int),
     "gpusw_measure_dpx_rate": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "gpusw_flush_l2": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+    "gpusw_locate_pairs": ([_VP, _I32, _I32, _VP, _VP, _I64, ctypes.c_int, _VP, _VP, _VP], ctypes.c_int),
     "gpusw_get_tune": ([_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _I32], ctypes.c_int),
     "gpusw_set_tune": ([_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _I32], ctypes.c_int),
     "gpusw_device_name": ([ctypes.c_int, ctypes.c_char_p, _I32], ctypes.c_int),
@@ -289,6 +290,16 @@ class Context:
         self._check(self.lib.gpusw_score_pairs(self.handle, qdb, rdb, _ptr(qi), _ptr(rj),
                                                qi.shape[0], DTYPE_CODES[dtype], _ptr(out)))
         return out
+
+    def locate_pairs(self, qdb: int, rdb: int, qi: np.ndarray, rj: np.ndarray, anchored: bool):
+        """(score, reference row, query column) of the first best cell of every pair."""
+        qi = np.ascontiguousarray(qi, dtype=np.int32)
+        rj = np.ascontiguousarray(rj, dtype=np.int32)
+        n = qi.shape[0]
+        sc, ri, qj = (np.empty(n, dtype=np.int32) for _ in range(3))
+        self._check(self.lib.gpusw_locate_pairs(self.handle, qdb, rdb, _ptr(qi), _ptr(rj), n,
+                                                int(bool(anchored)), _ptr(sc), _ptr(ri), _ptr(qj)))
+        return sc, ri, qj
 
     # ------------------------------------------------------------------- measurement
     def stats(self) -> Stats:

@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _native
 from .encode import Encoded, funnel
-from .errors import NoGpuError
+from .errors import GpuSWError, NoGpuError, SchemeError
 from .result import AlignResult
 from .scheme import Scheme
 
@@ -52,6 +52,17 @@ def _as_scheme(scheme) -> Scheme:
     if isinstance(scheme, str):
         return Scheme.preset(scheme)
     raise TypeError(f"scheme must be a Scheme or preset name, got {type(scheme).__name__}")
+
+
+def _reversed_prefixes(enc: Encoded, idx: np.ndarray, plen: np.ndarray):
+    """Codes and offsets of ``enc[idx[k]][:plen[k]]`` reversed, for every k."""
+    plen = plen.astype(np.int64)
+    offs = np.zeros(idx.shape[0] + 1, dtype=np.int64)
+    np.cumsum(plen, out=offs[1:])
+    last = np.asarray(enc.offsets, dtype=np.int64)[idx] + plen - 1
+    t = np.arange(offs[-1], dtype=np.int64) - np.repeat(offs[:-1], plen)
+    codes = np.asarray(enc.codes)[np.repeat(last, plen) - t]
+    return np.ascontiguousarray(codes, dtype=np.uint8), offs.astype(np.int32)
 
 
 class _DeviceSet:
@@ -203,6 +214,55 @@ class Aligner:
             self._record(ctx, "sw_cross")
         return AlignResult(None, self._queries.ids, self._refs.ids, self.scheme,
                            topk_idx=idx, topk_scores=sc)
+
+    def locate(self, qi, rj) -> dict:
+        """Coordinates of the best local alignment of the pairs ``(qi[k], rj[k])``.
+
+        Returns int32 arrays ``score``, ``query_start``, ``query_end``, ``ref_start``,
+        ``ref_end`` (0-based, end exclusive, ``-1`` where the score is 0). The end is the
+        first cell, in row-major order (reference row, then query column), that holds the
+        local maximum; the start comes from a second device pass, anchored at that end, over
+        the reversed prefixes -- its first best cell is the shortest optimal alignment. Both
+        passes are int32 dynamic programming on the device; no traceback matrix is kept.
+        The reference is score-only (its examples re-align hits on the CPU for
+        coordinates, ``examples/legacy_16s_gpu_align.py:280-292``); this is the device
+        counterpart, for local schemes.
+        """
+        if self.scheme.mode != "local":
+            raise SchemeError("locate() needs a local-mode scheme")
+        if self._refs is None or self._queries is None:
+            raise ValueError("call index(refs) and set_queries(queries) first")
+        qi = np.ascontiguousarray(qi, dtype=np.int32)
+        rj = np.ascontiguousarray(rj, dtype=np.int32)
+        if qi.shape != rj.shape or qi.ndim != 1:
+            raise ValueError("qi and rj must be 1-D and of the same length")
+        n = qi.shape[0]
+        res = {k: np.full(n, -1, dtype=np.int32)
+               for k in ("query_start", "query_end", "ref_start", "ref_end")}
+        ctx = self._ctx()
+        with ctx.lock:
+            ctx.set_scheme(self.scheme)
+            sc, rend, qend = ctx.locate_pairs(self._dq.handle, self._dref.handle, qi, rj, False)
+            res["score"] = sc
+            hit = np.flatnonzero(sc > 0)
+            if hit.size:
+                qrev = _reversed_prefixes(self._queries, qi[hit], qend[hit] + 1)
+                rrev = _reversed_prefixes(self._refs, rj[hit], rend[hit] + 1)
+                hq, hr = ctx.upload(*qrev), ctx.upload(*rrev)
+                try:
+                    ident = np.arange(hit.size, dtype=np.int32)
+                    sb, di, dj = ctx.locate_pairs(hq, hr, ident, ident, True)
+                finally:
+                    ctx.free(hq)
+                    ctx.free(hr)
+                if not np.array_equal(sb, sc[hit]):
+                    raise GpuSWError("anchored pass disagrees with the local score")
+                res["ref_start"][hit] = rend[hit] - di
+                res["query_start"][hit] = qend[hit] - dj
+                res["ref_end"][hit] = rend[hit] + 1
+                res["query_end"][hit] = qend[hit] + 1
+            self._record(ctx, "sw_locate")
+        return res
 
     # ----------------------------------------------------------------- introspection
     @property

@@ -163,6 +163,7 @@ struct RowFeed {
 
 // Per-lane accumulators of one task, merged over the column passes of the task.
 struct Acc {
+  int bi = 0x7FFFFFFF, bj = 0x7FFFFFFF;  // LOCATE: first cell (row-major) holding `best`
   uint32_t best;    // running max of HGO (local score / int16 overflow guard)
   uint32_t endrow;  // max over the last row of HGO at real columns   (non-local)
   uint32_t corner;  // HGO at (m, n)                                   (non-local)
@@ -190,7 +191,12 @@ struct Acc {
 // the last pass, so the end-column maximum costs one op per step instead of one per cell,
 // and the end row needs no column mask (the dummy columns hold 0, which the result takes
 // as a floor anyway).
-template <int G, int W, int P, bool LOCAL, bool PAIRS, bool LEFTPAD = false, class Feed = RowFeed>
+//
+// LOCATE (P = 1, local): instead of the 3-input running max, keep the first cell in
+// row-major order (reference row, then query column) that holds the maximum; across column
+// passes an equal value replaces the stored cell only if it comes earlier in that order.
+template <int G, int W, int P, bool LOCAL, bool PAIRS, bool LEFTPAD = false, class Feed = RowFeed,
+          bool LOCATE = false>
 __device__ __forceinline__ void team_pass(const SchemeDev& S, const uint4* __restrict__ prof,
                                           int pstride, const uint32_t* row_w0,
                                           const uint32_t* row_w1, int row_bits, int row_per,
@@ -304,8 +310,20 @@ __device__ __forceinline__ void team_pass(const SchemeDev& S, const uint4* __res
     }
     e_out = e;
     x_out = xlast;
+    if (LOCATE) {
 #pragma unroll
-    for (int k = 0; k + 1 < W; k += 2) acc.best = Ops::max3(acc.best, HGO[k], HGO[k + 1]);
+      for (int k = 0; k < W; ++k) {
+        const int v = (int)HGO[k], b = (int)acc.best, j = jbase + k;
+        if (j < n0 && (v > b || (v == b && (i < acc.bi || (i == acc.bi && j < acc.bj))))) {
+          acc.best = (uint32_t)v;
+          acc.bi = i;
+          acc.bj = j;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k + 1 < W; k += 2) acc.best = Ops::max3(acc.best, HGO[k], HGO[k + 1]);
+    }
     if (has_next && lane == G - 1) bnd[i] = make_uint2(e_out, x_out);
 
     if (LEFTPAD) {
@@ -417,6 +435,23 @@ __device__ __forceinline__ uint32_t team_max(uint32_t v, unsigned wmask) {
 #pragma unroll
   for (int off = G / 2; off > 0; off >>= 1) v = V<P>::max2(v, __shfl_xor_sync(wmask, v, off, G));
   return v;
+}
+
+// LOCATE reduction (int32): best value first, then the earliest (row, column).
+template <int G>
+__device__ __forceinline__ void team_argmax(Acc& a, unsigned wmask) {
+#pragma unroll
+  for (int off = G / 2; off > 0; off >>= 1) {
+    const int ov = (int)__shfl_xor_sync(wmask, a.best, off, G);
+    const int oi = __shfl_xor_sync(wmask, a.bi, off, G);
+    const int oj = __shfl_xor_sync(wmask, a.bj, off, G);
+    const int v = (int)a.best;
+    if (ov > v || (ov == v && (oi < a.bi || (oi == a.bi && oj < a.bj)))) {
+      a.best = (uint32_t)ov;
+      a.bi = oi;
+      a.bj = oj;
+    }
+  }
 }
 
 // Final score of half h from the team-reduced accumulators (HGO units: subtract go).

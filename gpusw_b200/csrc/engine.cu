@@ -333,9 +333,9 @@ int pair_teams(const Shape& s, int ns) {
   return std::max(1, t);
 }
 
-template <int G, int W, int P, bool L, bool LP>
+template <int G, int W, int P, bool L, bool LP, bool LOC = false>
 void launch_pairs_t(gpusw_ctx* c, Bufs& B, gsw::PairsParams prm, int /*teams_hint*/, long long max_rows, bool multipass) {
-  auto k = gsw::pairs_kernel<G, W, P, L, LP>;
+  auto k = gsw::pairs_kernel<G, W, P, L, LP, LOC>;
   const Shape s{G, W};
   const size_t sub_bytes = (size_t)gsw::pairs_sub_uint4(prm.S.ns) * 16;
   const size_t prof = profile_bytes(s, prm.S.ns);
@@ -1589,6 +1589,76 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
     if (n > 0) CK(cudaMemcpyAsync(out, B->out.p, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaEventRecord(c->ev3, c->stream));
     c->st.last_cells = cells;
+    c->st.last_pairs = n;
+    end_call(c);
+  });
+}
+
+int gpusw_locate_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi, const int32_t* rj,
+                       int64_t n, int anchored, int32_t* out_score, int32_t* out_rend,
+                       int32_t* out_qend) {
+  return guarded(c, [&] {
+    Db& q = get_db(c, qdb);
+    Db& r = get_db(c, rdb);
+    require_scheme(c, q, r);
+    if (!anchored && c->sch.mode != gsw::kModeLocal)
+      fail(GPUSW_ERR_SCHEME, "locating the best local alignment needs a local-mode scheme");
+    if (n < 0 || (n > 0 && (!qi || !rj || !out_score || !out_rend || !out_qend)))
+      fail(GPUSW_ERR_INVALID, "null arrays");
+    if (n >= (1ll << 31)) fail(GPUSW_ERR_INVALID, "at most 2^31 - 1 pairs per call");
+    int max_n = 0, max_m = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      if (qi[i] < 0 || qi[i] >= q.n || rj[i] < 0 || rj[i] >= r.n)
+        fail(GPUSW_ERR_INVALID, "pair index out of range at position " + std::to_string(i));
+      max_n = std::max(max_n, q.len[qi[i]]);
+      max_m = std::max(max_m, r.len[rj[i]]);
+    }
+    HostScheme h = c->sch;
+    if (anchored) {  // same table and gaps, both sequences anchored at their start
+      h.mode = gsw::kModeGlobal;
+      h.free_q = h.free_r = 0;
+    }
+    if (!width_ok(h, 1, max_n, max_m))
+      fail(GPUSW_ERR_OVERFLOW, "scores of this scheme and these lengths do not fit in int32");
+    begin_call(c);
+    CK(cudaEventRecord(c->ev1, c->stream));
+    if (n > 0) {
+      Bufs& B = c->shared;
+      B.reset_marks();
+      Staging stg;
+      const size_t o_qi = stg.add(qi, (size_t)n * 4), o_rj = stg.add(rj, (size_t)n * 4);
+      char* dm = stg.upload(c, B);
+      int* d_out = B.out.as<int>((size_t)n * 3);
+      unsigned long long* queue = B.queue.as<unsigned long long>(1);
+      CK(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), c->stream));
+      gsw::PairsParams pp{};
+      pp.S = make_scheme(h, 1);
+      pp.sub = c->sub_d;
+      pp.cols = q.packed();
+      pp.rows = r.packed();
+      pp.qi = reinterpret_cast<const int*>(dm + o_qi);
+      pp.rj = reinterpret_cast<const int*>(dm + o_rj);
+      pp.item_mode = 0;
+      pp.n_align = n;
+      pp.n_items = n;
+      pp.queue = queue;
+      pp.out = d_out;
+      pp.out_i = d_out + n;
+      pp.out_j = d_out + 2 * n;
+      const bool mp = max_n > kPairShapes[7].cap();
+      staged(c, B, false, [&] {
+        if (anchored) launch_pairs_t<32, 16, 1, false, false, true>(c, B, pp, 1, max_m, mp);
+        else launch_pairs_t<32, 16, 1, true, false, true>(c, B, pp, 1, max_m, mp);
+      });
+      c->last_bufs = &B;
+      CK(cudaEventRecord(c->ev2, c->stream));
+      CK(cudaMemcpyAsync(out_score, d_out, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync(out_rend, d_out + n, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync(out_qend, d_out + 2 * n, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
+    } else {
+      CK(cudaEventRecord(c->ev2, c->stream));
+    }
+    CK(cudaEventRecord(c->ev3, c->stream));
     c->st.last_pairs = n;
     end_call(c);
   });

@@ -179,6 +179,8 @@ struct PairsParams {
   Ovf* ovf;                  // int16 overflow output
   int* ovf_count;
   int ovf_cap;
+  int* out_i;                // LOCATE: row (reference) index of the best cell, or -1
+  int* out_j;                // LOCATE: column (query) index of the best cell, or -1
 };
 
 template <int P>
@@ -235,7 +237,7 @@ __host__ __device__ __forceinline__ int pairs_sub_uint4(int ns) {
   return ns <= kSubSmemMax ? (ns * ns + 3) / 4 : 0;
 }
 
-template <int G, int W, int P, bool LOCAL, bool LEFTPAD>
+template <int G, int W, int P, bool LOCAL, bool LEFTPAD, bool LOCATE = false>
 __global__ void __launch_bounds__(256) pairs_kernel(const PairsParams p) {
   extern __shared__ uint4 smem_prof[];
   constexpr int SLOTS = G * W / 4;
@@ -285,14 +287,26 @@ __global__ void __launch_bounds__(256) pairs_kernel(const PairsParams p) {
         build_profile_lane<G, W, P>(p.S, sub, p.cols, it.valid[0] ? it.q[0] : -1, n0, pad0,
                                     (P == 2 && it.valid[P - 1]) ? it.q[P - 1] : -1, n1, pad1,
                                     ps * G * W, prof, pstride, lane);
-        team_pass<G, W, P, LOCAL, true, LEFTPAD>(p.S, prof, pstride, w0, w1, p.rows.bits,
+        team_pass<G, W, P, LOCAL, true, LEFTPAD, RowFeed, LOCATE>(p.S, prof, pstride, w0, w1, p.rows.bits,
                                                  p.rows.per, m0, P == 2 ? m1 : m0,
                                                  LEFTPAD ? span : n0, LEFTPAD ? span : n1,
                                                  ps * G * W, bnd, ps > 0, ps + 1 < npass, lane,
                                                  wmask, acc, ps + 1 == npass);
         __syncwarp(wmask);
       }
-      acc = reduce_acc<G, P>(p.S, acc, wmask);
+      if (LOCATE) team_argmax<G>(acc, wmask);
+      else acc = reduce_acc<G, P>(p.S, acc, wmask);
+    }
+    if (LOCATE) {  // P == 1: the maximum over all cells and its first cell, row-major
+      if (lane == 0 && it.valid[0]) {
+        const bool cells = n[0] > 0 && m[0] > 0;
+        const int best = cells ? (int)acc.best - p.S.go : 0;
+        const bool hit = cells && (!LOCAL || best > 0);
+        p.out[it.pos[0]] = best;
+        p.out_i[it.pos[0]] = hit ? acc.bi : -1;
+        p.out_j[it.pos[0]] = hit ? acc.bj : -1;
+      }
+      continue;
     }
     if (lane == 0) {
 #pragma unroll

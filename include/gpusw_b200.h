@@ -123,6 +123,20 @@ int gpusw_topk(gpusw_ctx *ctx, int32_t qdb, int32_t rdb, const int32_t *qlist, i
 int gpusw_score_pairs(gpusw_ctx *ctx, int32_t qdb, int32_t rdb, const int32_t *qi,
                       const int32_t *rj, int64_t n, int dtype, int32_t *out);
 
+/* Best-cell coordinates of explicit pairs (int32): for every pair, out_score receives the
+ * maximum of H over all cells and out_rend/out_qend the 0-based reference row and query
+ * column of the first cell holding it in row-major order (reference row, then query
+ * column), or -1 when no cell scores above 0 in local mode. anchored = 0 runs the context's
+ * local scheme (the end of the best local alignment; out_score is then the local score);
+ * anchored = 1 runs the same table and gaps with both sequences anchored at their start
+ * (global boundaries, best cell anywhere) -- on reversed prefixes this gives the start of an
+ * optimal local alignment ending at a known cell. Replaces the CPU re-alignment the
+ * reference's examples use to recover coordinates (examples/legacy_16s_gpu_align.py:280-292,
+ * docs/DESIGN.md:95-96); the reference itself is score-only. */
+int gpusw_locate_pairs(gpusw_ctx *ctx, int32_t qdb, int32_t rdb, const int32_t *qi,
+                       const int32_t *rj, int64_t n, int anchored, int32_t *out_score,
+                       int32_t *out_rend, int32_t *out_qend);
+
 /* Engine options. plain != 0 selects the one-batch-per-call form (queries in input order,
  * one kernel shape per batch, no length binning, no graph) used as the comparison point
  * of the batched form. mem_budget bounds the score blocks of gpusw_topk (bytes, 0 keeps the

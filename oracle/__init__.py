@@ -7,6 +7,9 @@ import this package, and only to check or time against it. It holds:
   ``_score_codes`` (``src/gpusw/reference.py:38-125``), for small cases;
 * ``score_pairs`` / ``score_cross``: the same recurrence in plain C
   (``oracle/gotoh_oracle.c``), threaded over pairs, for large parity checks;
+* ``locate_pairs``: best-cell coordinates (end of the best local alignment, then its start
+  from an anchored pass over the reversed prefixes), the CPU restatement of the engine's
+  ``Aligner.locate`` (the reference is score-only);
 * ``topk_stable``: the reference's top-k order -- a stable sort of the negated scores,
   so ties go to the lower reference index (``src/gpusw/result.py:30-47``).
 
@@ -53,6 +56,8 @@ def _load():
         lib.oracle_score_cross.argtypes = [p, p, p, i64, p, p, i64, p, i32, i32, i32, i32, i32,
                                            i32, i32, p]
         lib.oracle_score_cross.restype = i32
+        lib.oracle_locate.argtypes = [p, i64, p, i64, p, i32, i32, i32, i32, p]
+        lib.oracle_locate.restype = i32
         _lib = lib
     return _lib
 
@@ -106,6 +111,48 @@ def score_cross(q_enc, r_enc, scheme, qlist=None, threads: int | None = None) ->
     if rc_ != 0:
         raise MemoryError("oracle ran out of memory")
     return out
+
+
+def locate_cells(qc, rc, scheme, anchored: bool) -> tuple[int, int, int]:
+    """(max H, reference row, query column) of the first best cell (C oracle, one pair)."""
+    lib = _load()
+    qc = np.ascontiguousarray(qc, dtype=np.uint8)
+    rc = np.ascontiguousarray(rc, dtype=np.uint8)
+    sub = np.ascontiguousarray(scheme.substitution_table(), dtype=np.int32)
+    out = np.zeros(3, dtype=np.int64)
+    if lib.oracle_locate(_ptr(qc), qc.shape[0], _ptr(rc), rc.shape[0], _ptr(sub),
+                         int(scheme.ns), int(scheme.gap_open), int(scheme.gap_extend),
+                         int(bool(anchored)), _ptr(out)) != 0:
+        raise MemoryError("oracle ran out of memory")
+    return int(out[0]), int(out[1]), int(out[2])
+
+
+def locate_pairs(q_enc, r_enc, qi, rj, scheme) -> dict:
+    """Coordinates of the best local alignment of every pair, half-open, -1 when score 0.
+
+    End: the first cell (row-major: reference row, then query column) holding the local
+    maximum. Start: the anchored pass over the reversed prefixes ending at that cell; its
+    first best cell, mapped back, is the start (the shortest such alignment).
+    """
+    qi = np.asarray(qi, dtype=np.int64)
+    rj = np.asarray(rj, dtype=np.int64)
+    n = qi.shape[0]
+    res = {k: np.full(n, -1, dtype=np.int64)
+           for k in ("query_start", "query_end", "ref_start", "ref_end")}
+    res["score"] = np.zeros(n, dtype=np.int64)
+    for k in range(n):
+        a, b = int(qi[k]), int(rj[k])
+        qc = q_enc.codes[q_enc.offsets[a]:q_enc.offsets[a + 1]]
+        rc = r_enc.codes[r_enc.offsets[b]:r_enc.offsets[b + 1]]
+        best, ie, je = locate_cells(qc, rc, scheme, anchored=False)
+        res["score"][k] = best
+        if best <= 0:
+            continue
+        rb, di, dj = locate_cells(qc[:je + 1][::-1], rc[:ie + 1][::-1], scheme, anchored=True)
+        assert rb == best
+        res["ref_start"][k], res["query_start"][k] = ie - di, je - dj
+        res["ref_end"][k], res["query_end"][k] = ie + 1, je + 1
+    return res
 
 
 def score_codes_py(qc, rc, sub, mode: str, go: int, ge: int, free_q: bool, free_r: bool) -> int:

@@ -17,6 +17,12 @@
  *   empty sequences                                            (reference.py:48-54)
  *
  * The pair loop is spread over POSIX threads; each pair is scored independently.
+ *
+ * oracle_locate adds the best-cell coordinates the engine's gpusw_locate_pairs returns (the
+ * reference is score-only; its examples re-align on the CPU to find coordinates,
+ * examples/legacy_16s_gpu_align.py:280-292): the same recurrence, local or anchored at the
+ * start (global boundaries), keeping the maximum of H over all cells and the first cell that
+ * holds it in row-major order (reference row, then query column).
  */
 #include <pthread.h>
 #include <stdint.h>
@@ -196,4 +202,40 @@ int oracle_score_cross(const uint8_t *qcodes, const int32_t *qoff, const int32_t
     job.maxq = max_len(qoff, qlist, nq, 0);
     if (nr == 0) return 0;
     return run_job(&job, nthreads);
+}
+
+/* out[0] = max of H over all cells; out[1], out[2] = 0-based reference row and query column
+ * of the first cell (row-major) holding it, or -1, -1 when no cell scores above 0 in local
+ * mode. anchored = 0: local; anchored = 1: global boundaries (both sequences start at their
+ * first residue), the end anywhere. Returns 0, or -1 when out of memory. */
+int oracle_locate(const uint8_t *q, int64_t n, const uint8_t *r, int64_t m, const int32_t *sub,
+                  int ns, int go, int ge, int anchored, int64_t *out) {
+    out[0] = 0; out[1] = -1; out[2] = -1;
+    if (n == 0 || m == 0) return 0;
+    int64_t *hp = (int64_t *)malloc(sizeof(int64_t) * 2 * (size_t)(n + 1));
+    if (!hp) return -1;
+    int64_t *f = hp + n + 1;
+    hp[0] = 0;
+    for (int64_t j = 1; j <= n; ++j) { hp[j] = anchored ? ladder(go, ge, j) : 0; f[j] = ORACLE_NEG; }
+    int64_t best = anchored ? ORACLE_NEG : 0, bi = -1, bj = -1;
+    for (int64_t i = 1; i <= m; ++i) {
+        const int32_t *subrow = sub + (int64_t)r[i - 1] * ns;
+        int64_t hleft = anchored ? ladder(go, ge, i) : 0, diag = hp[0], eleft = ORACLE_NEG;
+        hp[0] = hleft;
+        for (int64_t j = 1; j <= n; ++j) {
+            int64_t fj = hp[j] + go, fe = f[j] + ge;
+            if (fe > fj) fj = fe;
+            int64_t ej = hleft + go, ee = eleft + ge;
+            if (ee > ej) ej = ee;
+            int64_t h = diag + (int64_t)subrow[q[j - 1]];
+            if (ej > h) h = ej;
+            if (fj > h) h = fj;
+            if (!anchored && h < 0) h = 0;
+            if (h > best) { best = h; bi = i - 1; bj = j - 1; }
+            diag = hp[j]; hp[j] = h; f[j] = fj; hleft = h; eleft = ej;
+        }
+    }
+    free(hp);
+    out[0] = best; out[1] = bi; out[2] = bj;
+    return 0;
 }

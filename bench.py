@@ -371,7 +371,9 @@ def run_ours(args, rank, world, local):
         return ctx.stats()
 
     dpx = ctx.dpx_rate()
-    for _ in range(args.warmup):
+    # the engine records a call's plan as a CUDA graph on the second call with the same key
+    # and replays it from the third: at least two untimed calls precede the timed ones
+    for _ in range(max(args.warmup, 2)):
         step()
     sampler = ClockSampler(local)
     ctx.sync()
@@ -414,7 +416,7 @@ def run_ours(args, rank, world, local):
     # end to end through the C ABI with host buffers
     e2e_t = []
     h2d = d2h = 0
-    for _ in range(args.e2e_steps):
+    for it in range(args.e2e_steps + (1 if args.e2e_steps > 0 else 0)):  # one untimed warm-up
         ctx.sync()
         t0 = time.perf_counter()
         q2 = ctx.upload(*wl.queries)
@@ -427,7 +429,8 @@ def run_ours(args, rank, world, local):
             idx, sc = ctx.topk(q2, r2, qlist, wl.nr, wl.k, policy)
             d2h = idx.nbytes + sc.nbytes
             h2d_extra = qlist.nbytes
-        e2e_t.append(time.perf_counter() - t0)
+        if it > 0:
+            e2e_t.append(time.perf_counter() - t0)
         h2d = packed_bytes(wl.queries[1], ctx.bits(q2)) + packed_bytes(wl.refs[1], ctx.bits(r2)) + h2d_extra
         ctx.free(q2)
         ctx.free(r2)
@@ -436,6 +439,7 @@ def run_ours(args, rank, world, local):
         e_s = group.max(sum(e2e_t))
         e2e = {"value": world * cells * len(e2e_t) / e_s / 1e9, "unit": "GCUPS",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": [round(t * 1e3, 2) for t in e2e_t], "warmup": 1,
                "timing": "wall clock around upload + score + top-k + copy back"}
 
     # a short serving sweep over the same resident references (16S workload only)

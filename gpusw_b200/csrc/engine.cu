@@ -3,7 +3,11 @@
 // include/gpusw_b200.h.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdlib>
 #include <climits>
+#include <condition_variable>
+#include <functional>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -72,9 +76,12 @@ struct Db {
   std::vector<int> len;
   std::vector<long long> woff;
   std::vector<int> perm_desc;  // sequences by length, longest first (stable)
+  void* base = nullptr;        // one allocation: words, then woff_d, then len_d
   uint32_t* words = nullptr;
   long long* woff_d = nullptr;
   int* len_d = nullptr;
+  bool order_ready = false;    // perm_desc / perm_d / ident_d built (on first use as rows)
+  void* order_base = nullptr;  // one allocation: perm_d, then ident_d
   int* perm_d = nullptr;
   int* ident_d = nullptr;      // identity order (plain form)
   int64_t bytes = 0;
@@ -187,6 +194,7 @@ struct gpusw_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
   Bufs* last_bufs = nullptr;  // the set whose stage marks the last call used
   std::vector<std::unique_ptr<Plan>> plans;
+  std::vector<std::vector<long long>> seen_keys;  // cacheable keys run once, not yet recorded
   unsigned long long use_clock = 0;
   long long scheme_version = 0;
   int graphs = 1;              // replay cached plans as CUDA graphs
@@ -240,20 +248,122 @@ bool width_ok(const HostScheme& h, int P, long long max_n, long long max_m) {
   return true;
 }
 
+// Host phase timing, printed to stderr when the environment sets GPUSW_TRACE=1. Diagnostics
+// only: every phase runs the same with or without it.
+struct HostTrace {
+  using clk = std::chrono::steady_clock;
+  const char* call;
+  bool on;
+  clk::time_point last;
+  explicit HostTrace(const char* name) : call(name), on(enabled()), last(clk::now()) {}
+  static bool enabled() {
+    static const bool e = [] { const char* v = std::getenv("GPUSW_TRACE"); return v && v[0] == '1'; }();
+    return e;
+  }
+  void lap(const char* phase) {
+    if (!on) return;
+    const auto now = clk::now();
+    std::fprintf(stderr, "[gpusw] %s %s %.3f ms\n", call, phase,
+                 std::chrono::duration<double, std::milli>(now - last).count());
+    last = now;
+  }
+};
+
 // ------------------------------------------------------------------------- sequences
 int host_threads() { return (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency())); }
 
-// Run f(begin, end) over [0, n) split into contiguous ranges on the host's cores.
+// Persistent fork-join workers for the host-side passes (packing, scans, planning), so a call
+// does not pay thread creation. One job at a time; a caller that finds the pool busy (another
+// context's thread) spawns its own threads instead. Workers are never joined: they sleep on
+// the condition variable until the process ends.
+class HostPool {
+ public:
+  static HostPool& get() {
+    static HostPool* p = new HostPool();
+    return *p;
+  }
+  // Runs job(t) for t in [0, nt); job(0) on the calling thread. False if the pool is busy.
+  bool run(int nt, const std::function<void(int)>& job) {
+    std::unique_lock<std::mutex> busy(run_mu_, std::try_to_lock);
+    if (!busy.owns_lock()) return false;
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      while ((int)workers_.size() < nt - 1) {
+        const int id = (int)workers_.size();
+        workers_.emplace_back([this, id] { loop(id); });
+        workers_.back().detach();
+      }
+      job_ = &job;
+      active_ = nt - 1;
+      pending_ = nt - 1;
+      ++gen_;
+    }
+    cv_.notify_all();
+    job(0);
+    std::unique_lock<std::mutex> g(mu_);
+    done_.wait(g, [&] { return pending_ == 0; });
+    job_ = nullptr;
+    return true;
+  }
+
+ private:
+  void loop(int id) {
+    unsigned long long seen = 0;
+    for (;;) {
+      const std::function<void(int)>* job;
+      {
+        std::unique_lock<std::mutex> g(mu_);
+        cv_.wait(g, [&] { return gen_ != seen; });
+        seen = gen_;
+        if (id >= active_) continue;
+        job = job_;
+      }
+      (*job)(id + 1);
+      std::lock_guard<std::mutex> g(mu_);
+      if (--pending_ == 0) done_.notify_all();
+    }
+  }
+  std::mutex run_mu_, mu_;
+  std::condition_variable cv_, done_;
+  std::vector<std::thread> workers_;
+  const std::function<void(int)>* job_ = nullptr;
+  int active_ = 0, pending_ = 0;
+  unsigned long long gen_ = 0;
+};
+
+// Run f(begin, end) over [0, n) split into contiguous ranges on the host's cores (one range
+// when n is below `min_n`). The split depends only on n and the core count.
 template <class F>
-void parallel_ranges(long long n, F&& f) {
-  const int nt = n < (1 << 16) ? 1 : host_threads();
+void parallel_ranges_min(long long n, long long min_n, F&& f) {
+  const int nt = n < min_n ? 1 : (int)std::min<long long>(host_threads(), n);
   if (nt == 1) {
     f(0ll, n);
     return;
   }
+  const std::function<void(int)> job = [&](int t) { f(n * t / nt, n * (t + 1) / nt); };
+  if (HostPool::get().run(nt, job)) return;
   std::vector<std::thread> th;
-  for (int t = 0; t < nt; ++t) th.emplace_back([&, t] { f(n * t / nt, n * (t + 1) / nt); });
+  for (int t = 0; t < nt; ++t) th.emplace_back([&, t] { job(t); });
   for (auto& x : th) x.join();
+}
+
+template <class F>
+void parallel_ranges(long long n, F&& f) {
+  parallel_ranges_min(n, 1 << 16, std::forward<F>(f));
+}
+
+// Eight 2-bit codes, one per byte of x (byte e = code e), folded into 16 bits (code e at
+// bits 2e..2e+1): neighbouring fields are merged pairwise three times.
+inline uint32_t fold2(uint64_t x) {
+  x = (x | (x >> 6)) & 0x000F000F000F000Full;
+  x = (x | (x >> 12)) & 0x000000FF000000FFull;
+  return (uint32_t)((x | (x >> 24)) & 0xFFFFull);
+}
+// Eight 4-bit codes, one per byte, folded into 32 bits (code e at bits 4e..4e+3).
+inline uint32_t fold4(uint64_t x) {
+  x = (x | (x >> 4)) & 0x00FF00FF00FF00FFull;
+  x = (x | (x >> 8)) & 0x0000FFFF0000FFFFull;
+  return (uint32_t)(x | (x >> 16));
 }
 
 // Pack sequences [s0, s1) into words (each sequence's words including its alignment
@@ -264,8 +374,27 @@ void pack_range(const uint8_t* codes, const int32_t* offs, const Db& d, uint32_t
     const int len = d.len[s];
     uint32_t* dst = words + d.woff[s];
     const long long nw = (s + 1 < d.n ? d.woff[s + 1] : d.woff[s] + (((len + d.per - 1) / d.per + 3) & ~3ll)) - d.woff[s];
+    long long w = 0;
     int c = 0;
-    for (long long w = 0; w < nw; ++w) {
+    // Whole words of 2-, 4- and 8-bit codes: gather 8 code bytes per 64-bit load and fold
+    // neighbouring fields together (codes are below 2^bits, so no masking of the input).
+    if (d.bits == 2) {
+      for (; c + 16 <= len; c += 16, ++w) {
+        uint64_t a, b;
+        memcpy(&a, src + c, 8);
+        memcpy(&b, src + c + 8, 8);
+        dst[w] = fold2(a) | (fold2(b) << 16);
+      }
+    } else if (d.bits == 4) {
+      for (; c + 8 <= len; c += 8, ++w) {
+        uint64_t a;
+        memcpy(&a, src + c, 8);
+        dst[w] = fold4(a);
+      }
+    } else if (d.bits == 8) {
+      for (; c + 4 <= len; c += 4, ++w) memcpy(dst + w, src + c, 4);
+    }
+    for (; w < nw; ++w) {
       uint32_t v = 0;
       for (int e = 0; e < d.per && c < len; ++e, ++c) v |= (uint32_t)src[c] << (e * d.bits);
       dst[w] = v;
@@ -422,20 +551,40 @@ int pick_pair_shape(int ncols, int ns) {
   return 0;
 }
 
-// Host staging of several arrays into one device allocation.
+// Host staging of several arrays into one device allocation. `add` copies the bytes now;
+// `add_ref` only records the pointer, and the caller keeps that memory alive and unchanged
+// until `upload` has returned (the copies are issued from pageable memory, which the runtime
+// stages before cudaMemcpyAsync returns).
 struct Staging {
   std::vector<char> host;
+  struct Ref { size_t off; const void* src; size_t bytes; };
+  std::vector<Ref> refs;
+  size_t end = 0;
+  size_t place(size_t bytes) {
+    const size_t off = (end + 255) & ~(size_t)255;
+    end = off + bytes;
+    return off;
+  }
   size_t add(const void* src, size_t bytes) {
-    size_t off = (host.size() + 255) & ~(size_t)255;
-    host.resize(off + bytes);
+    const size_t off = place(bytes);
+    host.resize(end);
     if (bytes) memcpy(host.data() + off, src, bytes);
     return off;
   }
+  size_t add_ref(const void* src, size_t bytes) {
+    const size_t off = place(bytes);
+    if (bytes) refs.push_back({off, src, bytes});
+    return off;
+  }
   char* upload(gpusw_ctx* c, Bufs& B) {
-    char* d = static_cast<char*>(B.meta.get(std::max<size_t>(host.size(), 256)));
+    char* d = static_cast<char*>(B.meta.get(std::max<size_t>(end, 256)));
     // while recording a graph the plan's metadata is already in place from its eager run
-    if (!host.empty() && !B.capturing)
-      CK(cudaMemcpyAsync(d, host.data(), host.size(), cudaMemcpyHostToDevice, c->stream));
+    if (!B.capturing) {
+      if (!host.empty())
+        CK(cudaMemcpyAsync(d, host.data(), host.size(), cudaMemcpyHostToDevice, c->stream));
+      for (const Ref& r : refs)
+        CK(cudaMemcpyAsync(d + r.off, r.src, r.bytes, cudaMemcpyHostToDevice, c->stream));
+    }
     return d;
   }
 };
@@ -464,7 +613,34 @@ void run_cross(gpusw_ctx* c, Bufs& B, const Db& q, const Db& r, const int32_t* q
                int* out, long long out_ld);
 
 // Stream buffer of a reference set in sorted (batched) or input (plain) order.
+// Row order of a set used as references: longest first, stable (counting sort on the length),
+// and the identity order of the plain form, both on the device. Built on the set's first use
+// as references, before any graph capture of that use (every cached call runs eagerly first).
+void ensure_row_order(gpusw_ctx* c, Db& r) {
+  if (r.order_ready) return;
+  const int n = r.n;
+  r.perm_desc.resize(n);
+  {
+    std::vector<int> cnt((size_t)r.max_len + 2, 0);
+    for (int i = 0; i < n; ++i) cnt[(size_t)(r.max_len - r.len[i]) + 1]++;
+    for (size_t b = 1; b < cnt.size(); ++b) cnt[b] += cnt[b - 1];
+    for (int i = 0; i < n; ++i) r.perm_desc[cnt[(size_t)(r.max_len - r.len[i])]++] = i;
+  }
+  const size_t slots = (size_t)std::max(1, n);
+  std::vector<int> img(2 * slots, 0);
+  std::copy(r.perm_desc.begin(), r.perm_desc.end(), img.begin());
+  std::iota(img.begin() + slots, img.begin() + slots + n, 0);
+  CK(cudaMalloc(&r.order_base, img.size() * sizeof(int)));
+  r.perm_d = static_cast<int*>(r.order_base);
+  r.ident_d = r.perm_d + slots;
+  CK(cudaMemcpy(r.order_base, img.data(), img.size() * sizeof(int), cudaMemcpyHostToDevice));
+  r.bytes += (int64_t)(img.size() * sizeof(int));
+  c->held += (int64_t)(img.size() * sizeof(int));
+  r.order_ready = true;
+}
+
 const Db::Stream& get_stream(gpusw_ctx* c, Db& r, bool plain) {
+  ensure_row_order(c, r);
   const int pad = c->sch.ns;
   const std::pair<int, int> key(plain ? 1 : 0, pad);
   for (auto& kv : r.streams)
@@ -628,6 +804,7 @@ std::vector<double> run_autotune(gpusw_ctx* c, int P) {
   int32_t rdb = 0;
   if (gpusw_db_upload(c, rc.data(), ro.data(), nr, &rdb) != GPUSW_OK) fail(GPUSW_ERR_CUDA, c->err);
   Db& r = get_db(c, rdb);
+  ensure_row_order(c, r);
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -909,23 +1086,46 @@ int read_overflow_count(gpusw_ctx* c, Bufs& B) {
   return n;
 }
 
-// 64-bit hash of a byte range (8-byte words, multiply-xorshift mixing) for plan keys.
+// 64-bit hash of a byte range for plan keys: four interleaved multiply-xorshift lanes over
+// 8-byte words (independent chains, so the multiplies overlap), chunks of 1 MiB hashed on the
+// host's cores and their hashes chained in order. Not cryptographic; equal inputs give equal
+// keys within a process.
+uint64_t hash_chunk(const unsigned char* p, size_t bytes, uint64_t seed) {
+  uint64_t h[4] = {seed, seed ^ 0x243F6A8885A308D3ull, seed ^ 0x13198A2E03707344ull,
+                   seed ^ 0xA4093822299F31D0ull};
+  size_t i = 0;
+  for (; i + 32 <= bytes; i += 32) {
+    uint64_t w[4];
+    memcpy(w, p + i, 32);
+    for (int l = 0; l < 4; ++l) {
+      h[l] = (h[l] ^ w[l]) * 0x9E3779B97F4A7C15ull;
+      h[l] ^= h[l] >> 29;
+    }
+  }
+  uint64_t r = h[0] ^ (h[1] * 0xBF58476D1CE4E5B9ull) ^ (h[2] * 0x94D049BB133111EBull) ^ (h[3] >> 7);
+  for (; i < bytes; ++i) r = (r ^ p[i]) * 1099511628211ull;
+  return r ^ (uint64_t)bytes;
+}
+
 uint64_t fnv1a(const void* data, size_t bytes, uint64_t h = 1469598103934665603ull) {
   const unsigned char* p = static_cast<const unsigned char*>(data);
-  size_t i = 0;
-  for (; i + 8 <= bytes; i += 8) {
-    uint64_t w;
-    memcpy(&w, p + i, 8);
-    h = (h ^ w) * 0x9E3779B97F4A7C15ull;
-    h ^= h >> 29;
-  }
-  for (; i < bytes; ++i) h = (h ^ p[i]) * 1099511628211ull;
-  return h ^ (uint64_t)bytes;
+  constexpr size_t kChunk = 1 << 20;
+  if (bytes < 4 * kChunk) return hash_chunk(p, bytes, h);
+  const long long nch = (long long)((bytes + kChunk - 1) / kChunk);
+  std::vector<uint64_t> part((size_t)nch);
+  parallel_ranges_min(nch, 1, [&](long long lo, long long hi) {
+    for (long long k = lo; k < hi; ++k) {
+      const size_t o = (size_t)k * kChunk;
+      part[(size_t)k] = hash_chunk(p + o, std::min(kChunk, bytes - o), h + (uint64_t)k);
+    }
+  });
+  return hash_chunk(reinterpret_cast<const unsigned char*>(part.data()), part.size() * 8, h ^ bytes);
 }
 
 // Run `body` (the launches of one call) on the shared buffers, or through the plan of `key`:
-// the first time eagerly on the plan's own buffers and then recorded as a CUDA graph,
-// afterwards by replaying the graph. Returns the Bufs that hold the call's results.
+// the first time eagerly on the shared buffers, the second time eagerly on the plan's own
+// buffers and then recorded as a CUDA graph, afterwards by replaying the graph. Returns the
+// Bufs that hold the call's results.
 Plan* lookup(gpusw_ctx* c, const std::vector<long long>& key) {
   if (!c->graphs) return nullptr;
   for (auto& pl : c->plans)
@@ -951,6 +1151,18 @@ Bufs& execute(gpusw_ctx* c, const std::vector<long long>& key, bool cacheable, F
     return c->shared;
   }
   if (Plan* hit = lookup(c, key)) return replay(c, hit);
+  // A key met for the first time runs eagerly on the shared buffers; it is planned and
+  // recorded as a graph when it comes back, so one-off calls pay no capture.
+  auto seen = std::find(c->seen_keys.begin(), c->seen_keys.end(), key);
+  if (seen == c->seen_keys.end()) {
+    c->seen_keys.push_back(key);
+    if (c->seen_keys.size() > 16) c->seen_keys.erase(c->seen_keys.begin());
+    c->shared.reset_marks();
+    CK(cudaMemsetAsync(c->shared.ovf_flag.as<int>(1), 0, sizeof(int), c->stream));
+    body(c->shared);
+    return c->shared;
+  }
+  c->seen_keys.erase(seen);
   Plan* plan = nullptr;
   if (c->plans.size() >= 4) {  // evict the least recently used plan
     auto it = std::min_element(c->plans.begin(), c->plans.end(),
@@ -1165,11 +1377,8 @@ void gpusw_ctx_destroy(gpusw_ctx* c) {
       cudaFree(st.second.off);
       cudaFree(st.second.total);
     }
-    cudaFree(d.words);
-    cudaFree(d.woff_d);
-    cudaFree(d.len_d);
-    cudaFree(d.perm_d);
-    cudaFree(d.ident_d);
+    cudaFree(d.base);
+    cudaFree(d.order_base);
   }
   c->plans.clear();
   c->shared.release();
@@ -1221,82 +1430,119 @@ int gpusw_db_upload(gpusw_ctx* c, const uint8_t* codes, const int32_t* offsets, 
   return guarded(c, [&] {
     if (!offsets || !out_db || n < 0) fail(GPUSW_ERR_INVALID, "null offsets/handle or negative count");
     if (offsets[0] < 0) fail(GPUSW_ERR_INVALID, "offsets must be non-negative");
+    HostTrace tr("db_upload");
     auto d = std::make_unique<Db>();
     d->n = n;
     d->len.resize(n);
-    for (int i = 0; i < n; ++i) {
-      if (offsets[i + 1] < offsets[i]) fail(GPUSW_ERR_INVALID, "offsets must be non-decreasing");
-      d->len[i] = offsets[i + 1] - offsets[i];
-      d->max_len = std::max(d->max_len, d->len[i]);
+    const int nt = host_threads();
+    // lengths and their validation (threaded over sequences)
+    {
+      std::vector<int> tlen(nt + 1, 0), tbad(nt + 1, 0);
+      std::atomic<int> slot{0};
+      parallel_ranges(n, [&](long long lo, long long hi) {
+        int mx = 0, bad = 0;
+        for (long long i = lo; i < hi; ++i) {
+          const int l = offsets[i + 1] - offsets[i];
+          bad |= l < 0;
+          d->len[i] = l;
+          mx = std::max(mx, l);
+        }
+        const int t = slot++;
+        tlen[t] = mx;
+        tbad[t] = bad;
+      });
+      if (*std::max_element(tbad.begin(), tbad.end()))
+        fail(GPUSW_ERR_INVALID, "offsets must be non-decreasing");
+      d->max_len = *std::max_element(tlen.begin(), tlen.end());
     }
     const long long total = n ? (long long)offsets[n] - offsets[0] : 0;
     if (total > 0 && !codes) fail(GPUSW_ERR_INVALID, "null codes");
     // largest code (threaded) -> bits per residue
-    std::vector<int> tmax(host_threads() + 1, 0);
+    std::vector<int> tmax(nt + 1, 0);
     {
       const uint8_t* b0 = codes ? codes + offsets[0] : nullptr;
       std::atomic<int> slot{0};
       parallel_ranges(total, [&](long long lo, long long hi) {
-        int m = 0;
-        for (long long k = lo; k < hi; ++k) m = std::max<int>(m, b0[k]);
+        uint8_t m = 0;
+        for (long long k = lo; k < hi; ++k) m = std::max(m, b0[k]);
         tmax[slot++] = m;
       });
     }
     const int maxc = *std::max_element(tmax.begin(), tmax.end());
+    tr.lap("lengths+max");
     d->max_code = maxc;
     d->bits = maxc < 4 ? 2 : maxc < 16 ? 4 : maxc < 32 ? 5 : 8;
     d->per = d->bits == 5 ? 6 : 32 / d->bits;
     d->woff.resize(n);
     long long w = 0;
-    for (int i = 0; i < n; ++i) {
-      d->woff[i] = w;
-      w += ((d->len[i] + d->per - 1) / d->per + 3) & ~3ll;
+    {
+      // word offsets: every sequence starts on a 16-byte boundary (threaded two-pass scan)
+      const int per = d->per;
+      auto words_of = [per](int len) { return ((long long)(len + per - 1) / per + 3) & ~3ll; };
+      std::vector<std::pair<long long, long long>> span((size_t)nt + 1, {0, 0});
+      std::atomic<int> slot{0};
+      parallel_ranges(n, [&](long long lo, long long hi) {
+        long long sum = 0;
+        for (long long i = lo; i < hi; ++i) sum += words_of(d->len[i]);
+        span[slot++] = {lo, sum};
+      });
+      const int used = slot.load();
+      std::sort(span.begin(), span.begin() + used);
+      std::vector<std::pair<long long, long long>> start((size_t)used);
+      for (int t = 0; t < used; ++t) {
+        start[t] = {span[t].first, w};
+        w += span[t].second;
+      }
+      parallel_ranges(n, [&](long long lo, long long hi) {
+        // both passes split [0, n) the same way, so `lo` starts one of the first pass's ranges
+        auto it = std::lower_bound(start.begin(), start.end(), std::make_pair(lo, LLONG_MIN));
+        long long x = 0;
+        if (it != start.end() && it->first == lo) {
+          x = it->second;
+        } else {  // defensive: recount from the start
+          for (long long i = 0; i < lo; ++i) x += words_of(d->len[i]);
+        }
+        for (long long i = lo; i < hi; ++i) {
+          d->woff[i] = x;
+          x += words_of(d->len[i]);
+        }
+      });
     }
     const long long nwords = w + 64;  // tail slack for read-ahead
+    // one staging image and one device allocation: words | woff (8-byte) | len (4-byte)
+    const size_t words_b = (size_t)nwords * 4;
+    const size_t woff_o = (words_b + 255) & ~(size_t)255;
+    const size_t len_o = woff_o + (((size_t)std::max(1, n) * 8 + 255) & ~(size_t)255);
+    const size_t image_b = len_o + (size_t)std::max(1, n) * 4;
+    const size_t image_words = (image_b + 3) / 4;
     set_device(c);
     CK(cudaStreamSynchronize(c->stream));  // the staging buffer may still feed a copy
-    if ((size_t)nwords > c->pinned_words) {
+    if (image_words > c->pinned_words) {
       if (c->pinned) cudaFreeHost(c->pinned);
       c->pinned = nullptr;
       c->pinned_words = 0;
-      CK(cudaMallocHost(&c->pinned, (size_t)nwords * 4));
-      c->pinned_words = (size_t)nwords;
+      CK(cudaMallocHost(&c->pinned, image_words * 4));
+      c->pinned_words = image_words;
     }
+    tr.lap("offsets+pinned");
+    char* img = reinterpret_cast<char*>(c->pinned);
     // offsets are relative to codes[0] in the ABI (like the reference's Encoded)
     parallel_ranges(n, [&](long long lo, long long hi) { pack_range(codes, offsets, *d, c->pinned, (int)lo, (int)hi); });
     std::fill(c->pinned + w, c->pinned + nwords, 0u);
-    // longest first, stable: two-pass radix sort on the complemented length
-    d->perm_desc.resize(n);
-    {
-      std::vector<int> tmp(n);
-      std::iota(tmp.begin(), tmp.end(), 0);
-      std::vector<int> cnt(65537);
-      for (int pass = 0; pass < 2; ++pass) {
-        const int sh = pass * 16;
-        std::fill(cnt.begin(), cnt.end(), 0);
-        auto key = [&](int i) { return ((0x7FFFFFFFu - (uint32_t)d->len[i]) >> sh) & 0xFFFFu; };
-        for (int i = 0; i < n; ++i) cnt[key(tmp[i]) + 1]++;
-        for (int bk = 0; bk < 65536; ++bk) cnt[bk + 1] += cnt[bk];
-        for (int i = 0; i < n; ++i) d->perm_desc[cnt[key(tmp[i])]++] = tmp[i];
-        if (pass == 0) tmp.swap(d->perm_desc);
-      }
-    }
-    std::vector<int> ident(n);
-    std::iota(ident.begin(), ident.end(), 0);
-    CK(cudaMalloc(&d->words, nwords * sizeof(uint32_t)));
-    CK(cudaMalloc(&d->woff_d, std::max(1, n) * sizeof(long long)));
-    CK(cudaMalloc(&d->len_d, std::max(1, n) * sizeof(int)));
-    CK(cudaMalloc(&d->perm_d, std::max(1, n) * sizeof(int)));
-    CK(cudaMalloc(&d->ident_d, std::max(1, n) * sizeof(int)));
-    d->bytes = nwords * 4 + (long long)std::max(1, n) * 20;
-    CK(cudaMemcpyAsync(d->words, c->pinned, nwords * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
     if (n) {
-      CK(cudaMemcpyAsync(d->woff_d, d->woff.data(), n * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
-      CK(cudaMemcpyAsync(d->len_d, d->len.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-      CK(cudaMemcpyAsync(d->perm_d, d->perm_desc.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-      CK(cudaMemcpyAsync(d->ident_d, ident.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+      memcpy(img + woff_o, d->woff.data(), (size_t)n * 8);
+      memcpy(img + len_o, d->len.data(), (size_t)n * 4);
     }
+    tr.lap("pack");
+    CK(cudaMalloc(&d->base, image_b));
+    d->words = reinterpret_cast<uint32_t*>(d->base);
+    d->woff_d = reinterpret_cast<long long*>(static_cast<char*>(d->base) + woff_o);
+    d->len_d = reinterpret_cast<int*>(static_cast<char*>(d->base) + len_o);
+    d->bytes = (int64_t)image_b;
+    tr.lap("malloc");
+    CK(cudaMemcpyAsync(d->base, img, image_b, cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    tr.lap("copy");
     c->held += d->bytes;
     const int h = c->next_db++;
     c->dbs[h] = std::move(d);
@@ -1315,11 +1561,8 @@ int gpusw_db_free(gpusw_ctx* c, int32_t db) {
       cudaFree(st.second.total);
       c->held -= st.second.nbytes;
     }
-    cudaFree(d.words);
-    cudaFree(d.woff_d);
-    cudaFree(d.len_d);
-    cudaFree(d.perm_d);
-    cudaFree(d.ident_d);
+    cudaFree(d.base);
+    cudaFree(d.order_base);
     c->held -= d.bytes;
     c->dbs.erase(db);
   });
@@ -1337,6 +1580,7 @@ int gpusw_score_cross(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qli
     Db& q = get_db(c, qdb);
     Db& r = get_db(c, rdb);
     require_scheme(c, q, r);
+    ensure_row_order(c, r);
     if (nq < 0 || (nq > 0 && (!qlist || !out))) fail(GPUSW_ERR_INVALID, "null qlist/out");
     int max_n = 0;
     double qsum = 0;
@@ -1388,6 +1632,7 @@ int gpusw_topk(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qlist, int
     Db& q = get_db(c, qdb);
     Db& r = get_db(c, rdb);
     require_scheme(c, q, r);
+    ensure_row_order(c, r);
     if (k < 0) fail(GPUSW_ERR_INVALID, "k must be >= 0");
     if (nq < 0 || (nq > 0 && !qlist)) fail(GPUSW_ERR_INVALID, "null qlist");
     const int kk = std::min(k, r.n);
@@ -1472,14 +1717,36 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
     require_scheme(c, q, r);
     if (n < 0 || (n > 0 && (!qi || !rj || !out))) fail(GPUSW_ERR_INVALID, "null pair arrays");
     if (n >= (1ll << 31)) fail(GPUSW_ERR_INVALID, "at most 2^31 - 1 pairs per call");
+    HostTrace tr("score_pairs");
     int max_n = 0, max_m = 0;
     double cells = 0;
-    for (int64_t i = 0; i < n; ++i) {
-      if (qi[i] < 0 || qi[i] >= q.n || rj[i] < 0 || rj[i] >= r.n)
-        fail(GPUSW_ERR_INVALID, "pair index out of range at position " + std::to_string(i));
-      max_n = std::max(max_n, q.len[qi[i]]);
-      max_m = std::max(max_m, r.len[rj[i]]);
-      cells += (double)q.len[qi[i]] * r.len[rj[i]];
+    {
+      // validation and extents, threaded; the first bad position is reported
+      struct Part { int mn = 0, mm = 0; double cells = 0; int64_t bad = -1; };
+      std::vector<Part> part((size_t)host_threads() + 1);
+      std::atomic<int> slot{0};
+      parallel_ranges(n, [&](long long lo, long long hi) {
+        Part pt;
+        for (long long i = lo; i < hi; ++i) {
+          if (qi[i] < 0 || qi[i] >= q.n || rj[i] < 0 || rj[i] >= r.n) {
+            pt.bad = i;
+            break;
+          }
+          const int ql = q.len[qi[i]], rl = r.len[rj[i]];
+          pt.mn = std::max(pt.mn, ql);
+          pt.mm = std::max(pt.mm, rl);
+          pt.cells += (double)ql * rl;
+        }
+        part[slot++] = pt;
+      });
+      int64_t bad = -1;
+      for (const Part& pt : part) {
+        if (pt.bad >= 0 && (bad < 0 || pt.bad < bad)) bad = pt.bad;
+        max_n = std::max(max_n, pt.mn);
+        max_m = std::max(max_m, pt.mm);
+        cells += pt.cells;
+      }
+      if (bad >= 0) fail(GPUSW_ERR_INVALID, "pair index out of range at position " + std::to_string(bad));
     }
     begin_call(c);
     const HostScheme& h = c->sch;
@@ -1488,58 +1755,107 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
     const std::vector<long long> key = {2, qdb, rdb, c->scheme_version, P, c->plain, (long long)n, 0,
                                         (long long)fnv1a(rj, (size_t)n * 4, fnv1a(qi, (size_t)n * 4))};
     Bufs* B = nullptr;
+    tr.lap("validate+key");
     CK(cudaEventRecord(c->ev1, c->stream));
     // Plans the call on the host and runs it (recorded as a graph when cacheable).
     auto plan_and_run = [&](int Pw, bool cacheable) -> Bufs* {
-        // Plan (host, O(n)): kernel shape per alignment from its column length, then a
-        // stable two-pass radix order by (shape, row length descending) so int16x2
-        // partners share a shape and, mostly, a row length.
+        // Plan (host, O(n), threaded): kernel shape per alignment from its column length, then
+        // a stable order by (shape, row length descending) so int16x2 partners share a shape
+        // and, mostly, a row length: the input order when it already is one (checked), else a
+        // counting sort on that key (a two-pass radix sort when the key range is wide).
         std::vector<int> order((size_t)n);
         std::vector<uint8_t> shp((size_t)n);
         const int plain_shape = c->plain ? pick_pair_shape(std::max(1, max_n), h.ns) : 0;
-        {
-          std::vector<int> shape_of_len(4097);
-          for (int L = 0; L <= 4096; ++L) shape_of_len[L] = pick_pair_shape(std::max(1, L), h.ns);
-          const int big = pick_pair_shape(1 << 30, h.ns);
-          std::vector<uint32_t> keyv((size_t)n);
-          for (int64_t i = 0; i < n; ++i) {
-            const int ql = q.len[qi[i]];
-            shp[i] = (uint8_t)(c->plain ? plain_shape : (ql <= 4096 ? shape_of_len[ql] : big));
-            keyv[i] = ((uint32_t)shp[i] << 24) | (0xFFFFFFu - (uint32_t)std::min(r.len[rj[i]], 0xFFFFFF));
+        std::vector<int> shape_of_len(4097);
+        for (int L = 0; L <= 4096; ++L) shape_of_len[L] = pick_pair_shape(std::max(1, L), h.ns);
+        const int big = pick_pair_shape(1 << 30, h.ns);
+        struct Part {
+          long long lo = 0, hi = 0;
+          bool sorted = true;
+          int mrow[kNumPair] = {}, mcol[kNumPair] = {};
+          long long cnt[kNumPair] = {};
+        };
+        std::vector<Part> part((size_t)host_threads() + 1);
+        std::atomic<int> slot{0};
+        auto key_of = [&](int64_t i) {
+          return ((uint32_t)shp[i] << 24) | (0xFFFFFFu - (uint32_t)std::min(r.len[rj[i]], 0xFFFFFF));
+        };
+        parallel_ranges(n, [&](long long lo, long long hi) {
+          Part pt;
+          pt.lo = lo;
+          pt.hi = hi;
+          uint32_t prev = 0;
+          for (long long i = lo; i < hi; ++i) {
+            const int ql = q.len[qi[i]], rl = r.len[rj[i]];
+            const int sh = c->plain ? plain_shape : (ql <= 4096 ? shape_of_len[ql] : big);
+            shp[i] = (uint8_t)sh;
+            pt.mrow[sh] = std::max(pt.mrow[sh], rl);
+            pt.mcol[sh] = std::max(pt.mcol[sh], ql);
+            pt.cnt[sh]++;
+            const uint32_t k = key_of(i);
+            if (i > lo && k < prev) pt.sorted = false;
+            prev = k;
           }
-          if (c->plain) {
-            std::iota(order.begin(), order.end(), 0);
+          part[slot++] = pt;
+        });
+        const int used = slot.load();
+        std::sort(part.begin(), part.begin() + used, [](const Part& a, const Part& b) { return a.lo < b.lo; });
+        bool sorted = true;
+        int mrow[kNumPair] = {}, mcol[kNumPair] = {};
+        long long cnt[kNumPair] = {};
+        for (int t = 0; t < used; ++t) {
+          const Part& pt = part[t];
+          sorted &= pt.sorted;
+          if (t > 0 && pt.hi > pt.lo && part[t - 1].hi > part[t - 1].lo &&
+              key_of(pt.lo) < key_of(part[t - 1].hi - 1))
+            sorted = false;
+          for (int sh = 0; sh < kNumPair; ++sh) {
+            mrow[sh] = std::max(mrow[sh], pt.mrow[sh]);
+            mcol[sh] = std::max(mcol[sh], pt.mcol[sh]);
+            cnt[sh] += pt.cnt[sh];
+          }
+        }
+        if (c->plain || sorted) {
+          std::iota(order.begin(), order.end(), 0);
+        } else {
+          const int mm = std::min(max_m, 0xFFFFFF);
+          const size_t nb = (size_t)kNumPair * ((size_t)mm + 1);
+          if (nb <= (size_t)4 * n + 65536) {  // stable counting sort on (shape, mm - row length)
+            auto bucket = [&](int64_t i) {
+              return (size_t)shp[i] * ((size_t)mm + 1) + (size_t)(mm - std::min(r.len[rj[i]], 0xFFFFFF));
+            };
+            std::vector<int64_t> bc(nb + 1, 0);
+            for (int64_t i = 0; i < n; ++i) bc[bucket(i) + 1]++;
+            for (size_t bk = 0; bk < nb; ++bk) bc[bk + 1] += bc[bk];
+            for (int64_t i = 0; i < n; ++i) order[bc[bucket(i)]++] = (int)i;
           } else {
             std::vector<int> tmp((size_t)n);
             std::iota(tmp.begin(), tmp.end(), 0);
-            std::vector<int64_t> cnt(65537);
+            std::vector<int64_t> rc(65537);
             for (int pass = 0; pass < 2; ++pass) {
               const int sh = pass * 16;
-              std::fill(cnt.begin(), cnt.end(), 0);
-              for (int64_t i = 0; i < n; ++i) cnt[((keyv[tmp[i]] >> sh) & 0xFFFF) + 1]++;
-              for (int bkt = 0; bkt < 65536; ++bkt) cnt[bkt + 1] += cnt[bkt];
-              for (int64_t i = 0; i < n; ++i) order[cnt[(keyv[tmp[i]] >> sh) & 0xFFFF]++] = tmp[i];
+              std::fill(rc.begin(), rc.end(), 0);
+              for (int64_t i = 0; i < n; ++i) rc[((key_of(tmp[i]) >> sh) & 0xFFFF) + 1]++;
+              for (int bkt = 0; bkt < 65536; ++bkt) rc[bkt + 1] += rc[bkt];
+              for (int64_t i = 0; i < n; ++i) order[rc[(key_of(tmp[i]) >> sh) & 0xFFFF]++] = tmp[i];
               if (pass == 0) tmp.swap(order);
             }
           }
         }
         struct Bin { int64_t i0, i1; int shape, mrow, mcol; };
         std::vector<Bin> plan_bins;
-        for (int64_t i0 = 0; i0 < n;) {
-          const int sh = shp[order[i0]];
-          int64_t i1 = i0;
-          int mrow = 0, mcol = 0;
-          while (i1 < n && shp[order[i1]] == sh) {
-            mrow = std::max(mrow, r.len[rj[order[i1]]]);
-            mcol = std::max(mcol, q.len[qi[order[i1]]]);
-            ++i1;
+        {
+          int64_t i0 = 0;
+          for (int sh = 0; sh < kNumPair; ++sh) {
+            if (!cnt[sh]) continue;
+            plan_bins.push_back({i0, i0 + cnt[sh], sh, mrow[sh], mcol[sh]});
+            i0 += cnt[sh];
           }
-          plan_bins.push_back({i0, i1, sh, mrow, mcol});
-          i0 = i1;
         }
-        Staging stg;
-        const size_t o_qi = stg.add(qi, (size_t)n * 4), o_rj = stg.add(rj, (size_t)n * 4);
-        const size_t o_ord = stg.add(order.data(), (size_t)n * 4);
+        tr.lap("plan");
+        Staging stg;  // qi, rj and order stay alive until the eager run has uploaded them
+        const size_t o_qi = stg.add_ref(qi, (size_t)n * 4), o_rj = stg.add_ref(rj, (size_t)n * 4);
+        const size_t o_ord = stg.add_ref(order.data(), (size_t)n * 4);
         auto run = [&](int Pw) {
           return [&, Pw](Bufs& Bx) {
             char* dm = stg.upload(c, Bx);
@@ -1578,6 +1894,7 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
     if (n > 0) {
       Plan* hit = c->plain ? nullptr : lookup(c, key);
       B = hit ? &replay(c, hit) : plan_and_run(P, !c->plain);
+      tr.lap(hit ? "replay" : "run");
       if (P == 2) {
         const int n_ovf = read_overflow_count(c, *B);
         c->st.last_overflow = n_ovf;
@@ -1591,6 +1908,7 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
     c->st.last_cells = cells;
     c->st.last_pairs = n;
     end_call(c);
+    tr.lap("finish");
   });
 }
 

@@ -124,6 +124,7 @@ void slot_upload(Slot& sl) {
   }
   q.perm_desc.resize(n);
   std::iota(q.perm_desc.begin(), q.perm_desc.end(), 0);
+  q.order_ready = true;  // a query set: never used as references
   q.words = sl.words.as<uint32_t>((size_t)nwords);
   q.woff_d = sl.woff.as<long long>((size_t)std::max(1, n));
   q.len_d = sl.len.as<int>((size_t)std::max(1, n));
@@ -294,6 +295,7 @@ int gpusw_server_create(gpusw_ctx* ctx, int32_t rdb, int32_t k, int dtype, int64
   int rc = guarded(ctx, [&] {
     Db& r = get_db(ctx, rdb);
     if (!ctx->has_scheme) fail(GPUSW_ERR_SCHEME, "no scheme set");
+    ensure_row_order(ctx, r);
     if (r.max_code >= ctx->sch.ns) fail(GPUSW_ERR_INVALID, "reference codes exceed the scheme's table");
     if (k < 0 || max_slots < 1 || max_slots > 8 || max_batch_queries < 1 || max_pending < 1)
       fail(GPUSW_ERR_INVALID, "bad server limits");

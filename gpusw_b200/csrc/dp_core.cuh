@@ -281,10 +281,11 @@ __device__ __forceinline__ void team_pass(const SchemeDev& S, const uint4* __res
         const uint4 a = pr0[slot];
         if (PAIRS) {
           const uint4 b = pr1[slot];
-          sp[4 * k4 + 0] = (a.x & 0xFFFFu) | (b.x & 0xFFFF0000u);
-          sp[4 * k4 + 1] = (a.y & 0xFFFFu) | (b.y & 0xFFFF0000u);
-          sp[4 * k4 + 2] = (a.z & 0xFFFFu) | (b.z & 0xFFFF0000u);
-          sp[4 * k4 + 3] = (a.w & 0xFFFFu) | (b.w & 0xFFFF0000u);
+          // low half from a, high half from b: one byte permute per register
+          sp[4 * k4 + 0] = __byte_perm(a.x, b.x, 0x7610);
+          sp[4 * k4 + 1] = __byte_perm(a.y, b.y, 0x7610);
+          sp[4 * k4 + 2] = __byte_perm(a.z, b.z, 0x7610);
+          sp[4 * k4 + 3] = __byte_perm(a.w, b.w, 0x7610);
         } else {
           sp[4 * k4 + 0] = a.x;
           sp[4 * k4 + 1] = a.y;
@@ -452,6 +453,290 @@ __device__ __forceinline__ void team_argmax(Acc& a, unsigned wmask) {
       a.bj = oj;
     }
   }
+}
+
+// -------------------------------------------------------------------------------------
+// Explicit-pair column pass with a branch-free steady state (pairs kernel).
+//
+// Same recurrence, layout and packing as team_pass with PAIRS = true, restructured for the
+// read/window shapes where a team's per-row bookkeeping otherwise costs as much as its
+// cells:
+//  * Row codes come from a per-team ring in shared memory that already holds, for each row,
+//    the profile offsets of both halves (a half past its own end gets the pad row). Every
+//    lane reads the entry of its own row, so codes are neither shuffled nor decoded per
+//    step; the team refills half of the ring every kRingHalf steps.
+//  * Steps run in three stretches: the first G-1 (lanes still entering) and the rows from
+//    min(m0, m1) - 1 on (lanes leaving, last-row bookkeeping) take the checked path; in
+//    between every lane holds a real row of both halves, so the step has no branch.
+//  * The end column (LEFTPAD) is a per-lane running max merged by lane G-1 at the end.
+//  * The multi-pass boundary column is prefetched one row ahead by lane 0.
+// Not covered (team_pass is used instead): LOCATE, and the non-left-padded semiglobal mode
+// with free query ends, whose end column needs a mask per cell.
+constexpr int kRing = 128, kRingHalf = kRing / 2;
+
+// Code of row r of a packed sequence starting at word pointer w (per codes per word).
+__device__ __forceinline__ uint32_t packed_row_code(const uint32_t* w, int r, int bits, int per) {
+  unsigned q, rem;
+  if (per == 6) {
+    q = __umulhi((unsigned)r, 0xAAAAAAABu) >> 2;  // r / 6 for every 32-bit r
+    rem = (unsigned)r - q * 6u;
+  } else {
+    const int sh = __ffs(per) - 1;                 // per = 4, 8 or 16
+    q = (unsigned)r >> sh;
+    rem = (unsigned)r & (unsigned)(per - 1);
+  }
+  return (__ldg(w + q) >> (rem * (unsigned)bits)) & ((1u << bits) - 1u);
+}
+
+template <int G, int W, int P, bool LOCAL, bool LEFTPAD>
+struct FastPass {
+  using Ops = V<P>;
+  const SchemeDev& S;
+  const uint4* prof_lane;  // profile row 0, my slot
+  uint32_t* ring;
+  const uint32_t *w0, *w1;
+  int bits, per, pstride;
+  int m0, m1, mrows, n0, n1, jbase, lane;
+  unsigned wmask;
+  bool is_l0, is_last;
+  uint2* bnd;
+  uint32_t GO, GE, GES, NEGE0, NEGLOW, xb_step;
+  uint32_t HGO[W], F[W];
+  uint32_t hgo_left, e_out, x_out, xb, ec;
+  uint2 nb;  // lane 0, multi-pass: boundary of its next row
+
+  __device__ __forceinline__ FastPass(const SchemeDev& S_) : S(S_) {}
+
+  // ring entries of rows [r0, r1) (clipped to [0, mrows)), lane-strided
+  __device__ __forceinline__ void fill(int r0, int r1) {
+    r0 = max(r0, 0);
+    r1 = min(r1, mrows);
+    const uint32_t pad = (uint32_t)(S.pad_code * pstride);
+    for (int r = r0 + lane; r < r1; r += G) {
+      uint32_t a = pad, b = pad;
+      if (r < m0) a = packed_row_code(w0, r, bits, per) * (uint32_t)pstride;
+      if (P == 2 && r < m1) b = packed_row_code(w1, r, bits, per) * (uint32_t)pstride;
+      ring[r & (kRing - 1)] = a | (b << 16);
+    }
+  }
+
+  __device__ __forceinline__ void maybe_refill(int t) {
+    if (t > 0 && (t & (kRingHalf - 1)) == 0) {
+      __syncwarp(wmask);
+      fill(t + kRingHalf + 1 - G, t + kRing + 1 - G);
+      __syncwarp(wmask);
+    }
+  }
+
+  template <bool CHECKED, bool HP, bool HN, bool TRACK>
+  __device__ __forceinline__ void step(int t, Acc& acc) {
+    uint32_t e_in = __shfl_up_sync(wmask, e_out, 1, G);
+    uint32_t x_in = __shfl_up_sync(wmask, x_out, 1, G);
+    const int i = t - lane;  // my row (0-based)
+    if (HP) {
+      e_in = is_l0 ? nb.x : e_in;
+      x_in = is_l0 ? nb.y : x_in;
+      const int ni = t + 1;  // lane 0's next row
+      if (is_l0) nb = ni < mrows ? bnd[ni] : make_uint2(NEGE0, GO);
+    } else {
+      e_in = is_l0 ? NEGE0 : e_in;
+      x_in = is_l0 ? xb : x_in;
+    }
+    xb = Ops::add(xb, xb_step);
+    if (CHECKED && (unsigned)i >= (unsigned)mrows) return;
+
+    const uint32_t pc = ring[i & (kRing - 1)];
+    const uint4* pr0 = prof_lane + (pc & 0xFFFFu);
+    const uint4* pr1 = prof_lane + (pc >> 16);
+    constexpr int CH = (W % 16 == 0) ? 16 : ((W % 8 == 0) ? 8 : 4);
+    static_assert(W % CH == 0, "column chunks must tile W");
+    uint32_t diag = hgo_left;
+    uint32_t e = Ops::addmax(e_in, GES, x_in);
+    hgo_left = Ops::addmax(e_in, GO, x_in);
+    uint32_t xlast = 0;
+#pragma unroll
+    for (int c0 = 0; c0 < W; c0 += CH) {
+      uint32_t sp[CH];
+#pragma unroll
+      for (int k4 = 0; k4 < CH / 4; ++k4) {
+        const int slot = (c0 / 4 + k4) * G;
+        const uint4 a = pr0[slot];
+        if (P == 2) {
+          const uint4 b = pr1[slot];
+          // low half from a, high half from b: one byte permute per register
+          sp[4 * k4 + 0] = __byte_perm(a.x, b.x, 0x7610);
+          sp[4 * k4 + 1] = __byte_perm(a.y, b.y, 0x7610);
+          sp[4 * k4 + 2] = __byte_perm(a.z, b.z, 0x7610);
+          sp[4 * k4 + 3] = __byte_perm(a.w, b.w, 0x7610);
+        } else {
+          sp[4 * k4 + 0] = a.x;
+          sp[4 * k4 + 1] = a.y;
+          sp[4 * k4 + 2] = a.z;
+          sp[4 * k4 + 3] = a.w;
+        }
+      }
+      uint32_t XG[CH];
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        uint32_t f = Ops::addmax(F[c0 + k], GE, HGO[c0 + k]);
+        F[c0 + k] = f;
+        uint32_t x = LOCAL ? Ops::addmax_relu(diag, sp[k], f) : Ops::addmax(diag, sp[k], f);
+        diag = HGO[c0 + k];
+        XG[k] = Ops::add(x, GO);
+      }
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        HGO[c0 + k] = Ops::addmax(e, GO, XG[k]);
+        if (c0 + k + 1 < W) e = Ops::addmax(e, GES, XG[k]);
+      }
+      xlast = XG[CH - 1];
+    }
+    e_out = e;
+    x_out = xlast;
+    if (TRACK) {
+#pragma unroll
+      for (int k = 0; k + 1 < W; k += 2) acc.best = Ops::max3(acc.best, HGO[k], HGO[k + 1]);
+    }
+    if (HN && is_last) bnd[i] = make_uint2(e_out, x_out);
+
+    if (LEFTPAD) {
+      if (CHECKED) {
+        const uint32_t keep = (i < m0 ? Ops::half_mask(0) : 0u) | (i < m1 ? Ops::half_mask(1) : 0u);
+        ec = Ops::max2(ec, (HGO[W - 1] & keep) | (NEGLOW & ~keep));
+#pragma unroll
+        for (int h = 0; h < P; ++h) {
+          if (i == (h ? m1 : m0) - 1) {
+            const uint32_t hm = Ops::half_mask(h);
+            uint32_t v = acc.endrow;
+#pragma unroll
+            for (int k = 0; k < W; ++k) v = Ops::max2(v, HGO[k]);
+            acc.endrow = (acc.endrow & ~hm) | (v & hm);
+          }
+        }
+      } else {
+        ec = Ops::max2(ec, HGO[W - 1]);
+      }
+    } else if (!LOCAL && CHECKED) {
+      // last row of a half: the end row and the corner
+#pragma unroll
+      for (int h = 0; h < P; ++h) {
+        const int mh = h ? m1 : m0;
+        const int nh = h ? n1 : n0;
+        if (i == mh - 1) {
+          const uint32_t hm = Ops::half_mask(h);
+#pragma unroll
+          for (int k = 0; k < W; ++k) {
+            const int j = jbase + k;
+            if (j < nh) {
+              uint32_t v = Ops::max2(acc.endrow, HGO[k]);
+              acc.endrow = (acc.endrow & ~hm) | (v & hm);
+            }
+            if (j == nh - 1) acc.corner = (acc.corner & ~hm) | (HGO[k] & hm);
+          }
+        }
+      }
+    }
+  }
+
+  template <bool HP, bool HN, bool TRACK>
+  __device__ __forceinline__ void run(Acc& acc) {
+    const int mmin = P == 2 ? min(m0, m1) : m0;
+    const int nsteps = mrows + G - 1;
+    const int s0 = min(G - 1, nsteps), s1 = max(s0, mmin - 1);
+    int t = 0;
+    for (; t < s0; ++t) {
+      maybe_refill(t);
+      step<true, HP, HN, TRACK>(t, acc);
+    }
+    while (t < s1) {
+      maybe_refill(t);
+      const int te = min(s1, (t | (kRingHalf - 1)) + 1);
+#pragma unroll 1
+      for (; t < te; ++t) step<false, HP, HN, TRACK>(t, acc);
+    }
+    for (; t < nsteps; ++t) {
+      maybe_refill(t);
+      step<true, HP, HN, TRACK>(t, acc);
+    }
+  }
+};
+
+template <int G, int W, int P, bool LOCAL, bool LEFTPAD>
+__device__ __forceinline__ void team_pass_fast(const SchemeDev& S, const uint4* __restrict__ prof,
+                                               int pstride, uint32_t* ring,
+                                               const uint32_t* row_w0, const uint32_t* row_w1,
+                                               int row_bits, int row_per, int m0, int m1, int n0,
+                                               int n1, int col0, uint2* bnd, bool has_prev,
+                                               bool has_next, int lane, unsigned wmask, Acc& acc,
+                                               bool last_pass) {
+  using Ops = V<P>;
+  static_assert(W % 4 == 0, "W must be a multiple of 4");
+  FastPass<G, W, P, LOCAL, LEFTPAD> fp(S);
+  fp.prof_lane = prof + lane;
+  fp.ring = ring;
+  fp.w0 = row_w0;
+  fp.w1 = P == 2 ? row_w1 : row_w0;
+  fp.bits = row_bits;
+  fp.per = row_per;
+  fp.pstride = pstride;
+  fp.m0 = m0;
+  fp.m1 = P == 2 ? m1 : m0;
+  fp.mrows = P == 2 ? max(m0, m1) : m0;
+  fp.n0 = n0;
+  fp.n1 = n1;
+  fp.lane = lane;
+  fp.wmask = wmask;
+  fp.is_l0 = lane == 0;
+  fp.is_last = lane == G - 1;
+  fp.bnd = bnd;
+  fp.GO = Ops::splat(S.go);
+  fp.GE = Ops::splat(S.ge);
+  fp.GES = Ops::splat(S.ges);
+  fp.NEGE0 = Ops::splat(S.neg_e0);
+  fp.NEGLOW = Ops::splat(S.neg_low);
+  const bool ladder_row0 = !(S.mode == kModeLocal || (S.mode == kModeSemi && S.free_r));
+  const bool ladder_col0 = !(S.mode == kModeLocal || (S.mode == kModeSemi && S.free_q));
+  fp.jbase = col0 + lane * W;
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    const int h0 = ladder_row0 ? edge_value(S, false, fp.jbase + k + 1) : 0;
+    fp.HGO[k] = Ops::splat(h0 + S.go);
+    fp.F[k] = Ops::splat(S.neg_f);
+  }
+  fp.hgo_left = Ops::splat((ladder_row0 ? edge_value(S, false, fp.jbase) : 0) + S.go);
+  fp.e_out = fp.NEGE0;
+  fp.x_out = fp.GO;
+  fp.xb = Ops::splat((ladder_col0 ? S.go : 0) + S.go);
+  fp.xb_step = ladder_col0 ? fp.GE : 0u;
+  fp.ec = fp.NEGLOW;
+  fp.nb = make_uint2(fp.NEGE0, fp.GO);
+  if (has_prev && lane == 0 && fp.mrows > 0) fp.nb = bnd[0];
+  __syncwarp(wmask);
+  fp.fill(0, kRing + 1 - G);
+  __syncwarp(wmask);
+  // The running maximum is the local score, and in int16 the overflow guard; it is skipped
+  // where no cell can exceed the guard: outside local mode every H is at most
+  // min(n, m) * max(substitution score), since boundaries and gaps only subtract.
+  const int max_sub = 32767 - S.ovf_limit;
+  const bool track = LOCAL || (P == 2 && (long long)min(max(n0, n1), fp.mrows) * max_sub > S.ovf_limit);
+  if (track) {
+    if (has_prev) {
+      if (has_next) fp.template run<true, true, true>(acc);
+      else fp.template run<true, false, true>(acc);
+    } else {
+      if (has_next) fp.template run<false, true, true>(acc);
+      else fp.template run<false, false, true>(acc);
+    }
+  } else {
+    if (has_prev) {
+      if (has_next) fp.template run<true, true, false>(acc);
+      else fp.template run<true, false, false>(acc);
+    } else {
+      if (has_next) fp.template run<false, true, false>(acc);
+      else fp.template run<false, false, false>(acc);
+    }
+  }
+  if (LEFTPAD && last_pass && lane == G - 1) acc.endcol = Ops::max2(acc.endcol, fp.ec);
 }
 
 // Final score of half h from the team-reduced accumulators (HGO units: subtract go).

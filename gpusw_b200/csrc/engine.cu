@@ -467,7 +467,7 @@ void launch_pairs_t(gpusw_ctx* c, Bufs& B, gsw::PairsParams prm, int /*teams_hin
   auto k = gsw::pairs_kernel<G, W, P, L, LP, LOC>;
   const Shape s{G, W};
   const size_t sub_bytes = (size_t)gsw::pairs_sub_uint4(prm.S.ns) * 16;
-  const size_t prof = profile_bytes(s, prm.S.ns);
+  const size_t prof = profile_bytes(s, prm.S.ns) + gsw::kRing * sizeof(uint32_t);  // + row-code ring
   static int configured_dev = -1;
   static size_t configured_smem = 0;
   const size_t max_smem = 227 * 1024;

@@ -237,8 +237,10 @@ __host__ __device__ __forceinline__ int pairs_sub_uint4(int ns) {
   return ns <= kSubSmemMax ? (ns * ns + 3) / 4 : 0;
 }
 
+// At most 256 threads per block; one resident block is enough for the register budget, so
+// the compiler keeps every W-column state in registers (no spills in any instantiation).
 template <int G, int W, int P, bool LOCAL, bool LEFTPAD, bool LOCATE = false>
-__global__ void __launch_bounds__(256) pairs_kernel(const PairsParams p) {
+__global__ void __launch_bounds__(256, 1) pairs_kernel(const PairsParams p) {
   extern __shared__ uint4 smem_prof[];
   constexpr int SLOTS = G * W / 4;
   const int pstride = (SLOTS + 7) & ~7;
@@ -254,8 +256,12 @@ __global__ void __launch_bounds__(256) pairs_kernel(const PairsParams p) {
     __syncthreads();
     sub = s_sub;
   }
-  uint4* prof = smem_prof + sub_u4 + (size_t)team * (ns + 1) * pstride;
+  // per team: its profile, then its row-code ring (team_pass_fast)
+  uint4* prof = smem_prof + sub_u4 + (size_t)team * ((ns + 1) * pstride + kRing / 4);
+  uint32_t* ring = reinterpret_cast<uint32_t*>(prof + (ns + 1) * pstride);
   uint2* bnd = p.bnd ? p.bnd + ((size_t)blockIdx.x * nteams + team) * p.bnd_cap : nullptr;
+  // the branch-free pass covers every mode but the unpadded free-query-end semiglobal one
+  const bool fast = LOCAL || LEFTPAD || !(p.S.mode == kModeSemi && p.S.free_q);
   long long n_items = p.n_items;
   if (p.item_mode == 1) {
     n_items = min(*p.ovf_in_count, p.ovf_in_cap);
@@ -287,6 +293,17 @@ __global__ void __launch_bounds__(256) pairs_kernel(const PairsParams p) {
         build_profile_lane<G, W, P>(p.S, sub, p.cols, it.valid[0] ? it.q[0] : -1, n0, pad0,
                                     (P == 2 && it.valid[P - 1]) ? it.q[P - 1] : -1, n1, pad1,
                                     ps * G * W, prof, pstride, lane);
+        if constexpr (!LOCATE) {
+          if (fast) {
+            team_pass_fast<G, W, P, LOCAL, LEFTPAD>(p.S, prof, pstride, ring, w0, w1, p.rows.bits,
+                                                    p.rows.per, m0, P == 2 ? m1 : m0,
+                                                    LEFTPAD ? span : n0, LEFTPAD ? span : n1,
+                                                    ps * G * W, bnd, ps > 0, ps + 1 < npass, lane,
+                                                    wmask, acc, ps + 1 == npass);
+            __syncwarp(wmask);
+            continue;
+          }
+        }
         team_pass<G, W, P, LOCAL, true, LEFTPAD, RowFeed, LOCATE>(p.S, prof, pstride, w0, w1, p.rows.bits,
                                                  p.rows.per, m0, P == 2 ? m1 : m0,
                                                  LEFTPAD ? span : n0, LEFTPAD ? span : n1,

@@ -430,6 +430,55 @@ __device__ __forceinline__ void build_profile_lane(const SchemeDev& S, const int
   }
 }
 
+// Int8 form of build_profile_lane for two halves (P = 2, used when every profile value fits
+// in a signed byte): half h's values go to its own table profH, four columns per 32-bit
+// slot k4 * G + lane of each code row (pstride8 slots per row). Values as above.
+template <int G, int W, class Seqs = Packed>
+__device__ __forceinline__ void build_profile_lane8(const SchemeDev& S, const int* sub,
+                                                    const Seqs& cols, int c0, int n0, int pad0,
+                                                    int c1, int n1, int pad1, int col0,
+                                                    uint32_t* prof0, uint32_t* prof1,
+                                                    int pstride8, int lane) {
+  const int pad_s = S.s_pad - S.go, zero_s = -S.go;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int c = h ? c1 : c0, n = h ? n1 : n0, pd = h ? pad1 : pad0;
+    uint32_t* prof = h ? prof1 : prof0;
+    int code[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      const int j = col0 + lane * W + k - pd;  // real column, or < 0 (dummy) / >= n (past end)
+      code[k] = (c >= 0 && j >= 0 && j < n) ? cols.code(c, j) : (j < 0 ? -1 : -2);
+    }
+    for (int a = 0; a <= S.ns; ++a) {
+      uint32_t* row = prof + a * pstride8 + lane;
+#pragma unroll
+      for (int k4 = 0; k4 < W / 4; ++k4) {
+        uint32_t v = 0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int cd = code[4 * k4 + e];
+          const int hv = cd >= 0 ? (a < S.ns ? sub[a * S.ns + cd] - S.go : pad_s)
+                                 : (cd == -1 ? (a < S.ns ? zero_s : pad_s) : pad_s);
+          v |= (uint32_t)(hv & 0xFF) << (8 * e);
+        }
+        row[k4 * G] = v;
+      }
+    }
+  }
+}
+
+// Register e (0..3) of a 4-column group from the int8 tables: byte e of a (half 0) and of b
+// (half 1), each sign-extended to 16 bits, as one s16x2 word (one prmt with sign replication:
+// a selector nibble with bit 3 set yields the sign of the byte it names).
+template <int E>
+__device__ __forceinline__ uint32_t sx16x2(uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b),
+      "n"(E | ((8 | E) << 4) | ((4 + E) << 8) | ((12 + E) << 12)));
+  return d;
+}
+
 // Max-reduce an accumulator word over the G lanes of a team.
 template <int G, int P>
 __device__ __forceinline__ uint32_t team_max(uint32_t v, unsigned wmask) {
@@ -488,11 +537,13 @@ __device__ __forceinline__ uint32_t packed_row_code(const uint32_t* w, int r, in
   return (__ldg(w + q) >> (rem * (unsigned)bits)) & ((1u << bits) - 1u);
 }
 
-template <int G, int W, int P, bool LOCAL, bool LEFTPAD>
+template <int G, int W, int P, bool LOCAL, bool LEFTPAD, bool P8>
 struct FastPass {
   using Ops = V<P>;
   const SchemeDev& S;
   const uint4* prof_lane;  // profile row 0, my slot
+  const uint32_t* p8_lane0;  // P8: half 0's int8 table, row 0, my slot
+  const uint32_t* p8_lane1;  // P8: half 1's int8 table
   uint32_t* ring;
   const uint32_t *w0, *w1;
   int bits, per, pstride;
@@ -548,6 +599,8 @@ struct FastPass {
     const uint32_t pc = ring[i & (kRing - 1)];
     const uint4* pr0 = prof_lane + (pc & 0xFFFFu);
     const uint4* pr1 = prof_lane + (pc >> 16);
+    const uint32_t* q0 = p8_lane0 + (pc & 0xFFFFu);
+    const uint32_t* q1 = p8_lane1 + (pc >> 16);
     constexpr int CH = (W % 16 == 0) ? 16 : ((W % 8 == 0) ? 8 : 4);
     static_assert(W % CH == 0, "column chunks must tile W");
     uint32_t diag = hgo_left;
@@ -560,6 +613,14 @@ struct FastPass {
 #pragma unroll
       for (int k4 = 0; k4 < CH / 4; ++k4) {
         const int slot = (c0 / 4 + k4) * G;
+        if (P8) {
+          const uint32_t a = q0[slot], b = q1[slot];
+          sp[4 * k4 + 0] = sx16x2<0>(a, b);
+          sp[4 * k4 + 1] = sx16x2<1>(a, b);
+          sp[4 * k4 + 2] = sx16x2<2>(a, b);
+          sp[4 * k4 + 3] = sx16x2<3>(a, b);
+          continue;
+        }
         const uint4 a = pr0[slot];
         if (P == 2) {
           const uint4 b = pr1[slot];
@@ -661,8 +722,11 @@ struct FastPass {
   }
 };
 
-template <int G, int W, int P, bool LOCAL, bool LEFTPAD>
+// P8 (P = 2): the profile is the pair of int8 tables at prof8 (half 0) and prof8 +
+// (ns + 1) * pstride (half 1), pstride counting 32-bit slots; prof is unused.
+template <int G, int W, int P, bool LOCAL, bool LEFTPAD, bool P8 = false>
 __device__ __forceinline__ void team_pass_fast(const SchemeDev& S, const uint4* __restrict__ prof,
+                                               const uint32_t* prof8,
                                                int pstride, uint32_t* ring,
                                                const uint32_t* row_w0, const uint32_t* row_w1,
                                                int row_bits, int row_per, int m0, int m1, int n0,
@@ -671,8 +735,11 @@ __device__ __forceinline__ void team_pass_fast(const SchemeDev& S, const uint4* 
                                                bool last_pass) {
   using Ops = V<P>;
   static_assert(W % 4 == 0, "W must be a multiple of 4");
-  FastPass<G, W, P, LOCAL, LEFTPAD> fp(S);
+  static_assert(!P8 || P == 2, "int8 tables hold two halves");
+  FastPass<G, W, P, LOCAL, LEFTPAD, P8> fp(S);
   fp.prof_lane = prof + lane;
+  fp.p8_lane0 = prof8 + lane;
+  fp.p8_lane1 = prof8 + (S.ns + 1) * pstride + lane;
   fp.ring = ring;
   fp.w0 = row_w0;
   fp.w1 = P == 2 ? row_w1 : row_w0;

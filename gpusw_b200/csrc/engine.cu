@@ -462,12 +462,14 @@ int pair_teams(const Shape& s, int ns) {
   return std::max(1, t);
 }
 
-template <int G, int W, int P, bool L, bool LP, bool LOC = false>
+template <int G, int W, int P, bool L, bool LP, bool LOC = false, bool P8 = false>
 void launch_pairs_t(gpusw_ctx* c, Bufs& B, gsw::PairsParams prm, int /*teams_hint*/, long long max_rows, bool multipass) {
-  auto k = gsw::pairs_kernel<G, W, P, L, LP, LOC>;
+  auto k = gsw::pairs_kernel<G, W, P, L, LP, LOC, P8>;
   const Shape s{G, W};
   const size_t sub_bytes = (size_t)gsw::pairs_sub_uint4(prm.S.ns) * 16;
-  const size_t prof = profile_bytes(s, prm.S.ns) + gsw::kRing * sizeof(uint32_t);  // + row-code ring
+  // per team: the profile (s16x2, or two int8 tables of one byte per column) + row-code ring
+  const size_t prof = (P8 ? profile_bytes(s, prm.S.ns) / 2 : profile_bytes(s, prm.S.ns)) +
+                      gsw::kRing * sizeof(uint32_t);
   static int configured_dev = -1;
   static size_t configured_smem = 0;
   const size_t max_smem = 227 * 1024;
@@ -476,9 +478,16 @@ void launch_pairs_t(gpusw_ctx* c, Bufs& B, gsw::PairsParams prm, int /*teams_hin
     configured_smem = max_smem;
     configured_dev = c->device;
   }
-  // teams per block: the count that keeps the most warps resident (ties: larger blocks)
+  // teams per block: the count that keeps the most warps resident (ties: larger blocks),
+  // within the kernel's own thread limit
+  static int max_threads = 0;
+  if (!max_threads) {
+    cudaFuncAttributes fa{};
+    CK(cudaFuncGetAttributes(&fa, k));
+    max_threads = std::min(256, fa.maxThreadsPerBlock);
+  }
   int teams = 1, best_warps = -1, bps_best = 1;
-  for (int t = 1; t * G <= 256; t *= 2) {
+  for (int t = 1; t * G <= max_threads; t *= 2) {
     const size_t smem = sub_bytes + prof * t;
     if (smem > max_smem) break;
     int bps = 0;
@@ -507,17 +516,17 @@ void launch_pairs_t(gpusw_ctx* c, Bufs& B, gsw::PairsParams prm, int /*teams_hin
   c->st.last_launches++;
 }
 
-template <int P, bool L, bool LP>
+template <int P, bool L, bool LP, bool P8 = false>
 void launch_pairs_shape(gpusw_ctx* c, Bufs& B, int shape, const gsw::PairsParams& prm, int teams, long long max_rows, bool mp) {
   switch (shape) {
-    case 0: launch_pairs_t<8, 8, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
-    case 1: launch_pairs_t<8, 12, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
-    case 2: launch_pairs_t<8, 16, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
-    case 3: launch_pairs_t<8, 20, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
-    case 4: launch_pairs_t<8, 24, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
-    case 5: launch_pairs_t<16, 16, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
-    case 6: launch_pairs_t<16, 24, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
-    case 7: launch_pairs_t<32, 16, P, L, LP>(c, B, prm, teams, max_rows, mp); break;
+    case 0: launch_pairs_t<8, 8, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
+    case 1: launch_pairs_t<8, 12, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
+    case 2: launch_pairs_t<8, 16, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
+    case 3: launch_pairs_t<8, 20, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
+    case 4: launch_pairs_t<8, 24, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
+    case 5: launch_pairs_t<16, 16, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
+    case 6: launch_pairs_t<16, 24, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
+    case 7: launch_pairs_t<32, 16, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
     default: fail(GPUSW_ERR_INVALID, "bad pairs kernel shape");
   }
 }
@@ -527,6 +536,18 @@ void launch_pairs(gpusw_ctx* c, Bufs& B, int shape, int P, bool local, const gsw
   const int teams = pair_teams(kPairShapes[shape], prm.S.ns);
   const bool lp = prm.S.mode == gsw::kModeSemi && prm.S.free_q && prm.S.free_r;
   if (P == 2) {
+    // int8 query tables when every profile value (s - go, the pad score - go, -go) fits in
+    // a signed byte and the branch-free pass applies (all modes but the unpadded
+    // free-query-end semiglobal one)
+    const int max_sub = 32767 - prm.S.ovf_limit;  // max(0, largest substitution score)
+    const bool p8 = prm.S.s_pad - prm.S.go >= -128 && max_sub - prm.S.go <= 127 &&
+                    (local || lp || !(prm.S.mode == gsw::kModeSemi && prm.S.free_q));
+    if (p8) {
+      if (local) launch_pairs_shape<2, true, false, true>(c, B, shape, prm, teams, max_rows, multipass);
+      else if (lp) launch_pairs_shape<2, false, true, true>(c, B, shape, prm, teams, max_rows, multipass);
+      else launch_pairs_shape<2, false, false, true>(c, B, shape, prm, teams, max_rows, multipass);
+      return;
+    }
     if (local) launch_pairs_shape<2, true, false>(c, B, shape, prm, teams, max_rows, multipass);
     else if (lp) launch_pairs_shape<2, false, true>(c, B, shape, prm, teams, max_rows, multipass);
     else launch_pairs_shape<2, false, false>(c, B, shape, prm, teams, max_rows, multipass);

@@ -239,8 +239,12 @@ __host__ __device__ __forceinline__ int pairs_sub_uint4(int ns) {
 
 // At most 256 threads per block; one resident block is enough for the register budget, so
 // the compiler keeps every W-column state in registers (no spills in any instantiation).
-template <int G, int W, int P, bool LOCAL, bool LEFTPAD, bool LOCATE = false>
-__global__ void __launch_bounds__(256, 1) pairs_kernel(const PairsParams p) {
+//
+// P8 (P = 2, the branch-free pass only): the query profile is held as two int8 tables, half
+// the shared memory of the s16x2 table, and registers are capped at 128 (two 256-thread
+// blocks), so that more teams stay resident per SM.
+template <int G, int W, int P, bool LOCAL, bool LEFTPAD, bool LOCATE = false, bool P8 = false>
+__global__ void __launch_bounds__(256, P8 ? 2 : 1) pairs_kernel(const PairsParams p) {
   extern __shared__ uint4 smem_prof[];
   constexpr int SLOTS = G * W / 4;
   const int pstride = (SLOTS + 7) & ~7;
@@ -256,9 +260,11 @@ __global__ void __launch_bounds__(256, 1) pairs_kernel(const PairsParams p) {
     __syncthreads();
     sub = s_sub;
   }
-  // per team: its profile, then its row-code ring (team_pass_fast)
-  uint4* prof = smem_prof + sub_u4 + (size_t)team * ((ns + 1) * pstride + kRing / 4);
-  uint32_t* ring = reinterpret_cast<uint32_t*>(prof + (ns + 1) * pstride);
+  // per team: its profile (s16x2 table, or the two int8 tables), then its row-code ring
+  const size_t team_u4 = (P8 ? (size_t)(ns + 1) * pstride / 2 : (size_t)(ns + 1) * pstride) + kRing / 4;
+  uint4* prof = smem_prof + sub_u4 + (size_t)team * team_u4;
+  uint32_t* prof8 = reinterpret_cast<uint32_t*>(prof);
+  uint32_t* ring = reinterpret_cast<uint32_t*>(prof + team_u4 - kRing / 4);
   uint2* bnd = p.bnd ? p.bnd + ((size_t)blockIdx.x * nteams + team) * p.bnd_cap : nullptr;
   // the branch-free pass covers every mode but the unpadded free-query-end semiglobal one
   const bool fast = LOCAL || LEFTPAD || !(p.S.mode == kModeSemi && p.S.free_q);
@@ -290,12 +296,24 @@ __global__ void __launch_bounds__(256, 1) pairs_kernel(const PairsParams p) {
       const uint32_t* w0 = p.rows.words + p.rows.woff[max(it.r[0], 0)];
       const uint32_t* w1 = (P == 2 && it.r[P - 1] >= 0) ? p.rows.words + p.rows.woff[it.r[P - 1]] : w0;
       for (int ps = 0; ps < npass; ++ps) {
+        if constexpr (P8) {
+          build_profile_lane8<G, W>(p.S, sub, p.cols, it.valid[0] ? it.q[0] : -1, n0, pad0,
+                                    it.valid[P - 1] ? it.q[P - 1] : -1, n1, pad1, ps * G * W,
+                                    prof8, prof8 + (ns + 1) * pstride, pstride, lane);
+          team_pass_fast<G, W, P, LOCAL, LEFTPAD, true>(p.S, prof, prof8, pstride, ring, w0, w1,
+                                                        p.rows.bits, p.rows.per, m0, m1,
+                                                        LEFTPAD ? span : n0, LEFTPAD ? span : n1,
+                                                        ps * G * W, bnd, ps > 0, ps + 1 < npass,
+                                                        lane, wmask, acc, ps + 1 == npass);
+          __syncwarp(wmask);
+          continue;
+        }
         build_profile_lane<G, W, P>(p.S, sub, p.cols, it.valid[0] ? it.q[0] : -1, n0, pad0,
                                     (P == 2 && it.valid[P - 1]) ? it.q[P - 1] : -1, n1, pad1,
                                     ps * G * W, prof, pstride, lane);
         if constexpr (!LOCATE) {
           if (fast) {
-            team_pass_fast<G, W, P, LOCAL, LEFTPAD>(p.S, prof, pstride, ring, w0, w1, p.rows.bits,
+            team_pass_fast<G, W, P, LOCAL, LEFTPAD>(p.S, prof, prof8, pstride, ring, w0, w1, p.rows.bits,
                                                     p.rows.per, m0, P == 2 ? m1 : m0,
                                                     LEFTPAD ? span : n0, LEFTPAD ? span : n1,
                                                     ps * G * W, bnd, ps > 0, ps + 1 < npass, lane,

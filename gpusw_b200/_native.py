@@ -20,7 +20,7 @@ __all__ = ["LIB_PATH", "load", "gpu_available", "Context", "context", "Stats", "
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libgpusw_sm100.so")
 
 OK, E_INVALID, E_NO_GPU, E_CUDA, E_MEMORY, E_OVERFLOW, E_SCHEME = 0, 1, 2, 3, 4, 5, 6
-E_QUEUE_FULL, E_NOT_FOUND, E_CANCELLED, E_TIMEOUT = 7, 8, 9, 10
+E_QUEUE_FULL, E_NOT_FOUND, E_CANCELLED, E_TIMEOUT, E_UNSUPPORTED = 7, 8, 9, 10, 11
 DTYPE_CODES = {"auto": 0, "int16": 1, "int32": 2}
 MODE_CODES = {"local": 0, "global": 1, "semiglobal": 2}
 
@@ -102,6 +102,17 @@ _SIGNATURES = {
     "gpusw_server_get_stats": ([_VP, ctypes.POINTER(ServerStats)], ctypes.c_int),
     "gpusw_server_last_error": ([_VP], ctypes.c_char_p),
     "gpusw_server_destroy": ([_VP], None),
+    "gpusw_fasta_parse": ([ctypes.c_char_p, _I64, _VP, _I32, ctypes.c_int, ctypes.POINTER(_VP)], ctypes.c_int),
+    "gpusw_fasta_count": ([_VP], _I32),
+    "gpusw_fasta_residues": ([_VP], _I64),
+    "gpusw_fasta_codes": ([_VP], _VP),
+    "gpusw_fasta_offsets": ([_VP], _VP),
+    "gpusw_fasta_ids": ([_VP], _VP),
+    "gpusw_fasta_id_offsets": ([_VP], _VP),
+    "gpusw_fasta_error": ([_VP], ctypes.c_char_p),
+    "gpusw_fasta_bad_record": ([_VP], _I64),
+    "gpusw_fasta_bad_byte": ([_VP], _I32),
+    "gpusw_fasta_free": ([_VP], None),
 }
 
 
@@ -121,6 +132,47 @@ def load():
                 fn.restype = res
             _lib = lib
     return _lib
+
+
+def parse_fasta(data: bytes, lut: np.ndarray, sentinel: int, unknown_error: bool):
+    """FASTA bytes -> (codes uint8, offsets int32, ids) through the native reader, or None
+    when the text needs the Unicode reader (a byte >= 0x80, vertical tab, form feed or a
+    byte 0x1c-0x1f).
+
+    Raises ``ValueError`` with attributes ``bad_record`` / ``bad_byte`` for an
+    out-of-alphabet symbol (unknown="error") or a set beyond 2**31 - 1 residues.
+    Needs no GPU.
+    """
+    lib = load()
+    lut = np.ascontiguousarray(lut, dtype=np.uint8)
+    h = ctypes.c_void_p()
+    rc = lib.gpusw_fasta_parse(data, len(data), _ptr(lut), int(sentinel), int(bool(unknown_error)),
+                               ctypes.byref(h))
+    try:
+        if rc == E_UNSUPPORTED:
+            return None
+        if rc != OK:
+            err = ValueError(lib.gpusw_fasta_error(h).decode() if h.value else f"status {rc}")
+            err.bad_record = int(lib.gpusw_fasta_bad_record(h)) if h.value else -1
+            err.bad_byte = int(lib.gpusw_fasta_bad_byte(h)) if h.value else -1
+            raise err
+        n = int(lib.gpusw_fasta_count(h))
+        total = int(lib.gpusw_fasta_residues(h))
+        codes = np.empty(total, dtype=np.uint8)
+        if total:
+            ctypes.memmove(codes.ctypes.data, lib.gpusw_fasta_codes(h), total)
+        offsets = np.empty(n + 1, dtype=np.int32)
+        ctypes.memmove(offsets.ctypes.data, lib.gpusw_fasta_offsets(h), 4 * (n + 1))
+        id_off = np.ctypeslib.as_array(ctypes.cast(lib.gpusw_fasta_id_offsets(h), ctypes.POINTER(ctypes.c_int64)),
+                                       shape=(n + 1,))
+        nbytes = int(id_off[-1])
+        blob = ctypes.string_at(lib.gpusw_fasta_ids(h), nbytes).decode("ascii") if nbytes else ""
+        bounds = id_off.tolist()
+        ids = [blob[bounds[k]:bounds[k + 1]] for k in range(n)]
+        return codes, offsets, ids
+    finally:
+        if h.value:
+            lib.gpusw_fasta_free(h)
 
 
 def gpu_available() -> bool:

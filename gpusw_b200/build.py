@@ -10,7 +10,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc", "engine.cu")
-DEPS = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "dp_core.cuh", "kernels.cuh", "server.cuh")]
+DEPS = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "dp_core.cuh", "kernels.cuh", "server.cuh", "fasta.cuh")]
 HEADER = os.path.join(os.path.dirname(HERE), "include", "gpusw_b200.h")
 OUT = os.path.join(HERE, "libgpusw_sm100.so")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",

@@ -2289,3 +2289,4 @@ extern "C" int gpusw_score_pairs_noalloc(const uint8_t* q_codes, const int32_t* 
 }
 
 #include "server.cuh"
+#include "fasta.cuh"

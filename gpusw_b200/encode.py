@@ -21,7 +21,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .errors import EncodeError
+from .errors import EncodeError, NoGpuError
 
 __all__ = ["Encoded", "funnel", "build_lut", "read_fasta"]
 
@@ -171,8 +171,48 @@ def encode_pairs(pairs, scheme) -> Encoded:
                    lengths.astype(np.int32), scheme.eff_alphabet)
 
 
+def _fasta_bytes(obj: str):
+    """The FASTA bytes behind a str input (a path, ``.gz`` too, or FASTA text), else None."""
+    if os.path.exists(obj):
+        with open(obj, "rb") as fh:
+            data = fh.read()
+        return gzip.decompress(data) if obj.endswith(".gz") else data
+    if obj.lstrip().startswith(">"):
+        try:
+            return obj.encode("ascii")
+        except UnicodeEncodeError:
+            return None
+    return None
+
+
+def _encode_fasta_native(data: bytes, scheme) -> Encoded | None:
+    """FASTA bytes -> Encoded in one native pass (the engine library's reader; no GPU
+    needed). None when the library is not built or the text needs the Unicode reader; an
+    out-of-alphabet symbol is also left to the Python path, which words the error."""
+    try:
+        from . import _native
+
+        lut, sentinel = build_lut(scheme)
+        res = _native.parse_fasta(data, lut, sentinel, scheme.unknown == "error")
+    except (ImportError, OSError, NoGpuError):  # the library is not built
+        return None
+    except ValueError as exc:
+        if getattr(exc, "bad_record", -1) >= 0:
+            return None
+        raise EncodeError(str(exc)) from None
+    if res is None:
+        return None
+    codes, offsets, ids = res
+    return Encoded(codes, offsets, ids, np.diff(offsets).astype(np.int32), scheme.eff_alphabet)
+
+
 def funnel(obj, scheme, *, id_prefix: str = "q") -> Encoded:
-    """Turn any accepted input into an :class:`Encoded` for ``scheme``."""
+    """Turn any accepted input into an :class:`Encoded` for ``scheme``.
+
+    FASTA paths and FASTA text go through the engine library's native reader when it is
+    built and the text is plain ASCII (one pass: lines, ids, table lookup); everything else,
+    and those when the native reader declines, through the Python reader below. Both give
+    the same records, codes and errors."""
     if isinstance(obj, Encoded):
         if obj.alphabet != scheme.eff_alphabet:
             raise EncodeError(
@@ -183,4 +223,10 @@ def funnel(obj, scheme, *, id_prefix: str = "q") -> Encoded:
     if (isinstance(obj, tuple) and len(obj) in (2, 3) and isinstance(obj[0], np.ndarray)
             and isinstance(obj[1], np.ndarray) and obj[0].dtype == np.uint8):
         return _pre_encoded(obj, scheme, id_prefix)
+    if isinstance(obj, str):
+        data = _fasta_bytes(obj)
+        if data is not None:
+            enc = _encode_fasta_native(data, scheme)
+            if enc is not None:
+                return enc
     return encode_pairs(_to_pairs(obj, id_prefix), scheme)

@@ -33,6 +33,7 @@ extern "C" {
 #define GPUSW_ERR_NOT_FOUND 8    /* unknown handle or request id */
 #define GPUSW_ERR_CANCELLED 9    /* serving: the request was cancelled */
 #define GPUSW_ERR_TIMEOUT 10     /* a bounded wait ran out */
+#define GPUSW_ERR_UNSUPPORTED 11 /* input this routine does not take (the caller uses its own) */
 
 /* Alignment modes (src/gpusw/scheme.py:19, MODES). */
 #define GPUSW_MODE_LOCAL 0
@@ -276,6 +277,29 @@ const char *gpusw_server_last_error(const gpusw_server *srv);
 
 /* Stop the scheduler (waiting at most for the in-flight batches) and free the server. */
 void gpusw_server_destroy(gpusw_server *srv);
+
+/* ------------------------------------------------------------------ FASTA (host only)
+ * Native reader and encoder for FASTA text, replacing the reference's Python reader and
+ * per-sequence encoding loop (src/gpusw/encode.py:89-120, :196-225) with one pass over
+ * the bytes; no CUDA call, so it also runs without a GPU. `lut` is the scheme's 256-entry
+ * code table (case folding included) and `sentinel` its out-of-alphabet code; with
+ * unknown_error != 0 the first byte mapping to the sentinel fails the parse with
+ * GPUSW_ERR_INVALID, and gpusw_fasta_bad_record / _bad_byte name it. Text with a byte
+ * >= 0x80 or one of \v \f \x1c-\x1f returns GPUSW_ERR_UNSUPPORTED (the caller's Unicode
+ * reader handles it). On any return *out, when set, must be freed with gpusw_fasta_free. */
+typedef struct gpusw_fasta gpusw_fasta;
+int gpusw_fasta_parse(const char *data, int64_t len, const uint8_t *lut, int32_t sentinel,
+                      int unknown_error, gpusw_fasta **out);
+int32_t gpusw_fasta_count(const gpusw_fasta *f);            /* records */
+int64_t gpusw_fasta_residues(const gpusw_fasta *f);         /* total codes */
+const uint8_t *gpusw_fasta_codes(const gpusw_fasta *f);     /* residues codes */
+const int32_t *gpusw_fasta_offsets(const gpusw_fasta *f);   /* count + 1 offsets */
+const char *gpusw_fasta_ids(const gpusw_fasta *f);          /* ids, concatenated */
+const int64_t *gpusw_fasta_id_offsets(const gpusw_fasta *f); /* count + 1 offsets into ids */
+const char *gpusw_fasta_error(const gpusw_fasta *f);
+int64_t gpusw_fasta_bad_record(const gpusw_fasta *f);
+int32_t gpusw_fasta_bad_byte(const gpusw_fasta *f);
+void gpusw_fasta_free(gpusw_fasta *f);
 
 #ifdef __cplusplus
 }

@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="16s",
                     choices=["16s", "protein", "pairs", "small", "serving"])
+    ap.add_argument("--serve-slots", type=int, default=2)
+    ap.add_argument("--serve-batch-cells", type=float, default=0.0,
+                    help="server work per batch in cells (0: the engine default)")
     ap.add_argument("--serve-loads", default="1,4,16",
                     help="offered loads (requests/s) of the serving sweep")
     ap.add_argument("--serve-requests", type=int, default=8, help="requests per offered load")
@@ -277,7 +280,7 @@ def packed_bytes(offs: np.ndarray, bits: int) -> int:
     return int(words.sum() * 4 + 64 * 4 + lens.shape[0] * 20)
 
 
-def serving_sweep(aligner, loads, n_requests, seed=4, slots=2, k=10):
+def serving_sweep(aligner, loads, n_requests, seed=4, slots=2, k=10, batch_cells=0.0):
     """Poisson request stream at each offered load against the resident references of
     `aligner`; latencies (submit -> done) and sustained GCUPS come from the native server."""
     import threading
@@ -293,7 +296,7 @@ def serving_sweep(aligner, loads, n_requests, seed=4, slots=2, k=10):
     rng = np.random.default_rng(seed + 1)
     out = []
     for lam in loads:
-        with Server(aligner, k=k, slots=slots, max_batch_queries=1024) as srv:
+        with Server(aligner, k=k, slots=slots, max_batch_queries=1024, batch_cells=batch_cells) as srv:
             gaps = rng.exponential(1.0 / lam, size=len(encs))
             ids, done = [], []
 
@@ -337,7 +340,8 @@ def run_serving(args, rank, world, local):
                    wl.scheme.eff_alphabet)
     al = Aligner(wl.scheme, device=local).index(refs)
     loads = [float(x) for x in args.serve_loads.split(",")]
-    sweep = serving_sweep(al, loads, args.serve_requests)
+    sweep = serving_sweep(al, loads, args.serve_requests, slots=args.serve_slots,
+                          batch_cells=args.serve_batch_cells)
     if rank == 0:
         top = max(sweep, key=lambda r: r["gcups"])
         print(json.dumps({"metric": METRIC, "value": top["gcups"], "unit": "GCUPS", "n_gpus": world,
@@ -346,6 +350,8 @@ def run_serving(args, rank, world, local):
                           "data": "synthetic",
                           "config": {"workload": "serving over the resident 16S reference set, top-10",
                                      "refs": wl.nr, "requests_per_load": args.serve_requests,
+                                     "slots": args.serve_slots,
+                                     "batch_cells": args.serve_batch_cells or "engine default",
                                      "request_queries": "1-512 log-uniform, lengths U[50,2000]"},
                           "serving": sweep}), flush=True)
 
@@ -452,7 +458,8 @@ def run_ours(args, rank, world, local):
                        np.diff(wl.refs[1]).astype(np.int32), wl.scheme.eff_alphabet)
         al = Aligner(wl.scheme, device=local).index(refs)
         serving = serving_sweep(al, [float(x) for x in args.serve_loads.split(",")],
-                                args.serve_requests)
+                                args.serve_requests, slots=args.serve_slots,
+                                batch_cells=args.serve_batch_cells)
         del al
 
     # CPU oracle baseline and a bit-exact check of the same sample (rank 0, N = 1)

@@ -102,6 +102,7 @@ _SIGNATURES = {
     "gpusw_server_get_stats": ([_VP, ctypes.POINTER(ServerStats)], ctypes.c_int),
     "gpusw_server_last_error": ([_VP], ctypes.c_char_p),
     "gpusw_server_destroy": ([_VP], None),
+    "gpusw_server_set_batch_cells": ([_VP, ctypes.c_double], ctypes.c_int),
     "gpusw_fasta_parse": ([ctypes.c_char_p, _I64, _VP, _I32, ctypes.c_int, ctypes.POINTER(_VP)], ctypes.c_int),
     "gpusw_fasta_count": ([_VP], _I32),
     "gpusw_fasta_residues": ([_VP], _I64),

@@ -3,11 +3,17 @@
 //
 // Threads: callers submit/poll/cancel under `mu`; one scheduler thread owns the slots.
 // Each slot is a private context (own CUDA stream and buffers) that borrows the owner's
-// resident reference set; a batch is the concatenated queries of the requests admitted
-// together, scored by one planned launch sequence followed by the top-k kernel, with the
-// results copied into pinned host memory and an event recorded. The scheduler polls the
-// events (no device-side waits anywhere), splits finished batches per request and admits
-// the next requests in arrival order while a slot and the memory budget allow.
+// resident reference set; a batch is the concatenated queries of the request parts
+// admitted together, scored by one planned launch sequence followed by the top-k kernel,
+// with the results copied into pinned host memory and an event recorded. The scheduler
+// polls the events (no device-side waits anywhere), copies finished parts into their
+// requests and admits more work while a slot and the memory budget allow.
+//
+// Batches are cut by work, not by request: a batch holds about batch_cells cells, and
+// while other requests wait no request takes more than half of it, so a large request runs
+// as several parts and small requests that arrive behind it share the next batch instead of
+// waiting for it to finish (chunked, fair-share continuous batching). Requests are still
+// served in arrival order; a request completes when its last part does.
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -22,9 +28,15 @@ double now_ms() {
   return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
 }
 
+// Default target work per batch (gpusw_server_set_batch_cells changes it).
+constexpr double kServeBatchCells = 3e12;
+
 struct SrvRequest {
   int64_t id = 0;
   int nq = 0;
+  int next_q = 0;   // queries handed to batches so far
+  int parts = 0;    // parts in flight
+  bool failed = false;
   std::vector<uint8_t> codes;
   std::vector<int32_t> offsets;  // rebased to 0, nq + 1 entries
   int state = GPUSW_REQ_PENDING;
@@ -40,8 +52,8 @@ struct Slot {
   Db q;                          // the batch's query set (storage below, grow-only)
   DevBuf words, woff, len, perm, ident;
   std::vector<uint32_t> hwords;
-  std::vector<SrvRequest*> batch;
-  std::vector<int> row0;
+  struct Part { SrvRequest* r; int q0, nq, row0; };
+  std::vector<Part> parts;
   int nq = 0, P = 2;
   int64_t bytes = 0;
   cudaEvent_t done = nullptr;
@@ -58,6 +70,8 @@ struct gpusw_server {
   gpusw_ctx* owner = nullptr;
   Db* refs = nullptr;
   int kk = 0, dtype = 0;
+  double ref_residues = 0;  // total length of the resident references
+  double batch_cells = kServeBatchCells;
   int64_t budget = 4ll << 30, in_use = 0;
   int max_slots = 2, max_batch = 1024, max_pending = 4096;
   std::vector<std::unique_ptr<Slot>> slots;
@@ -86,18 +100,19 @@ void slot_upload(Slot& sl) {
   gpusw_ctx* c = sl.ctx;
   Db& q = sl.q;
   int n = 0, maxc = 0;
-  for (SrvRequest* r : sl.batch) n += r->nq;
+  for (const Slot::Part& pt : sl.parts) n += pt.nq;
   q.n = n;
   q.len.assign(n, 0);
   q.woff.assign(n, 0);
   q.max_len = 0;
   int i = 0;
-  for (SrvRequest* r : sl.batch) {
-    for (int a = 0; a < r->nq; ++a, ++i) {
+  for (const Slot::Part& pt : sl.parts) {
+    const SrvRequest* r = pt.r;
+    for (int a = pt.q0; a < pt.q0 + pt.nq; ++a, ++i) {
       q.len[i] = r->offsets[a + 1] - r->offsets[a];
       q.max_len = std::max(q.max_len, q.len[i]);
+      for (int c = r->offsets[a]; c < r->offsets[a + 1]; ++c) maxc = std::max<int>(maxc, r->codes[c]);
     }
-    for (uint8_t v : r->codes) maxc = std::max<int>(maxc, v);
   }
   q.max_code = maxc;
   q.bits = maxc < 4 ? 2 : maxc < 16 ? 4 : maxc < 32 ? 5 : 8;
@@ -110,8 +125,9 @@ void slot_upload(Slot& sl) {
   const long long nwords = w + 64;
   sl.hwords.assign((size_t)nwords, 0u);
   i = 0;
-  for (SrvRequest* r : sl.batch) {
-    for (int a = 0; a < r->nq; ++a, ++i) {
+  for (const Slot::Part& pt : sl.parts) {
+    const SrvRequest* r = pt.r;
+    for (int a = pt.q0; a < pt.q0 + pt.nq; ++a, ++i) {
       const uint8_t* src = r->codes.data() + r->offsets[a];
       uint32_t* dst = sl.hwords.data() + q.woff[i];
       for (int cidx = 0; cidx < q.len[i]; cidx += q.per) {
@@ -194,17 +210,26 @@ void server_loop(gpusw_server* s) {
       }
       const double t = now_ms();
       const int kk = s->kk;
-      for (size_t b = 0; b < sl.batch.size(); ++b) {
-        SrvRequest* r = sl.batch[b];
+      for (const Slot::Part& pt : sl.parts) {
+        SrvRequest* r = pt.r;
+        --r->parts;
         if (!fail_msg.empty()) {
-          r->state = GPUSW_REQ_FAILED;
+          r->failed = true;
           s->worker_err = fail_msg;
+        } else if (!r->cancel && kk > 0) {
+          std::copy(sl.h_idx + (size_t)pt.row0 * kk, sl.h_idx + (size_t)(pt.row0 + pt.nq) * kk,
+                    r->idx.begin() + (size_t)pt.q0 * kk);
+          std::copy(sl.h_sc + (size_t)pt.row0 * kk, sl.h_sc + (size_t)(pt.row0 + pt.nq) * kk,
+                    r->sc.begin() + (size_t)pt.q0 * kk);
+        }
+        if (r->parts > 0 || (r->next_q < r->nq && !r->cancel && !r->failed)) continue;
+        // the request's last part is back
+        if (r->failed) {
+          r->state = GPUSW_REQ_FAILED;
         } else if (r->cancel) {
           r->state = GPUSW_REQ_CANCELLED;
           ++s->cancelled;
         } else {
-          r->idx.assign(sl.h_idx + (size_t)sl.row0[b] * kk, sl.h_idx + (size_t)(sl.row0[b] + r->nq) * kk);
-          r->sc.assign(sl.h_sc + (size_t)sl.row0[b] * kk, sl.h_sc + (size_t)(sl.row0[b] + r->nq) * kk);
           r->state = GPUSW_REQ_DONE;
           r->t_done = t;
           s->lat.push_back(t - r->t_submit);
@@ -214,38 +239,59 @@ void server_loop(gpusw_server* s) {
         r->codes.clear();
         r->codes.shrink_to_fit();
       }
-      sl.batch.clear();
+      sl.parts.clear();
       sl.busy = false;
       s->in_use -= sl.bytes;
       progressed = true;
     }
     if (progressed) s->done_cv.notify_all();
-    // admissions, in arrival order
+    // admissions: parts of the pending requests, in arrival order, cut by work
     for (auto& slp : s->slots) {
       Slot& sl = *slp;
       if (sl.busy || s->pending.empty() || s->stop) continue;
       int64_t bytes = 0;
       int nq = 0, max_len = 0;
-      std::vector<SrvRequest*> take;
-      while (!s->pending.empty()) {
-        SrvRequest* r = s->pending.front();
-        if (!take.empty() && nq + r->nq > s->max_batch) break;
-        if (s->in_use + bytes + r->bytes > s->budget) break;
-        take.push_back(r);
-        s->pending.pop_front();
-        bytes += r->bytes;
-        nq += r->nq;
-        max_len = std::max(max_len, r->max_len);
+      double cells = 0;
+      std::vector<Slot::Part> take;
+      // with company in the queue no request takes more than half a batch
+      const double share = s->pending.size() > 1 ? s->batch_cells / 2 : s->batch_cells;
+      for (size_t qi = 0; qi < s->pending.size() && nq < s->max_batch && cells < s->batch_cells;) {
+        SrvRequest* r = s->pending[qi];
+        Slot::Part pt{r, r->next_q, 0, nq};
+        double rcells = 0;
+        int64_t rbytes = 0;
+        while (r->next_q < r->nq && nq < s->max_batch) {
+          const int a = r->next_q;
+          const int len = r->offsets[a + 1] - r->offsets[a];
+          const double qc = (double)len * s->ref_residues;
+          const int64_t qb = request_bytes(s, 1, len);
+          const bool first = take.empty() && pt.nq == 0;
+          if (!first && (rcells + qc > share || cells + qc > s->batch_cells)) break;
+          if (s->in_use + bytes + rbytes + qb > s->budget) break;
+          rcells += qc;
+          rbytes += qb;
+          ++pt.nq;
+          ++nq;
+          ++r->next_q;
+          max_len = std::max(max_len, len);
+        }
+        if (pt.nq == 0) break;  // budget or batch full: the rest waits
+        cells += rcells;
+        bytes += rbytes;
+        take.push_back(pt);
+        ++r->parts;
+        if (r->state == GPUSW_REQ_PENDING) {
+          r->state = GPUSW_REQ_RUNNING;
+          if (s->kk > 0) {
+            r->idx.assign((size_t)r->nq * s->kk, 0);
+            r->sc.assign((size_t)r->nq * s->kk, 0);
+          }
+        }
+        if (r->next_q == r->nq) s->pending.erase(s->pending.begin() + (long)qi);
+        else ++qi;
       }
       if (take.empty()) break;  // the head request waits for memory to free up
-      sl.batch = take;
-      sl.row0.clear();
-      int row = 0;
-      for (SrvRequest* r : take) {
-        sl.row0.push_back(row);
-        row += r->nq;
-        r->state = GPUSW_REQ_RUNNING;
-      }
+      sl.parts = take;
       sl.bytes = bytes;
       s->in_use += bytes;
       sl.busy = true;
@@ -263,9 +309,13 @@ void server_loop(gpusw_server* s) {
       }
       lk.lock();
       if (!fail_msg.empty()) {  // the batch failed before reaching the device
-        for (SrvRequest* r : sl.batch) r->state = GPUSW_REQ_FAILED;
+        for (const Slot::Part& pt : sl.parts) {
+          pt.r->failed = true;
+          s->pending.erase(std::remove(s->pending.begin(), s->pending.end(), pt.r), s->pending.end());
+          if (--pt.r->parts == 0) pt.r->state = GPUSW_REQ_FAILED;
+        }
         s->worker_err = fail_msg;
-        sl.batch.clear();
+        sl.parts.clear();
         sl.busy = false;
         s->in_use -= sl.bytes;
         s->done_cv.notify_all();
@@ -302,6 +352,7 @@ int gpusw_server_create(gpusw_ctx* ctx, int32_t rdb, int32_t k, int dtype, int64
     srv->owner = ctx;
     srv->refs = &r;
     srv->kk = std::min(k, r.n);
+    for (int l : r.len) srv->ref_residues += l;
     srv->dtype = dtype;
     if (mem_budget > 0) srv->budget = mem_budget;
     srv->max_slots = max_slots;
@@ -451,7 +502,16 @@ int gpusw_server_cancel(gpusw_server* s, int64_t req_id) {
     ++s->cancelled;
     s->done_cv.notify_all();
   } else if (r->state == GPUSW_REQ_RUNNING) {
+    // parts not yet handed out are dropped; the request ends when its last part is back,
+    // or now if none is on the device
     r->cancel = true;
+    s->pending.erase(std::remove(s->pending.begin(), s->pending.end(), r), s->pending.end());
+    if (r->parts == 0) {
+      r->state = GPUSW_REQ_CANCELLED;
+      ++s->cancelled;
+      r->codes.clear();
+      s->done_cv.notify_all();
+    }
   }
   return GPUSW_OK;
 }
@@ -466,7 +526,7 @@ int gpusw_server_get_stats(gpusw_server* s, gpusw_server_stats* out) {
   st.rejected = s->rejected;
   st.pending = (int64_t)s->pending.size();
   for (auto& sl : s->slots)
-    if (sl->busy) st.running += (int64_t)sl->batch.size();
+    if (sl->busy) st.running += (int64_t)sl->parts.size();
   st.batches = s->batches;
   st.mean_batch_queries = s->batches ? (double)s->batch_q / s->batches : 0.0;
   if (!s->lat.empty()) {
@@ -486,6 +546,13 @@ int gpusw_server_get_stats(gpusw_server* s, gpusw_server_stats* out) {
   st.gcups = st.wall_s > 0 ? s->cells / st.wall_s / 1e9 : 0.0;
   for (auto& sl : s->slots) st.device_bytes += sl->ctx->held;
   *out = st;
+  return GPUSW_OK;
+}
+
+int gpusw_server_set_batch_cells(gpusw_server* s, double cells) {
+  if (!s || cells < 0) return GPUSW_ERR_INVALID;
+  std::lock_guard<std::mutex> g(s->mu);
+  s->batch_cells = cells > 0 ? cells : kServeBatchCells;
   return GPUSW_OK;
 }
 

@@ -37,7 +37,8 @@ class Server:
     """
 
     def __init__(self, aligner, k: int = 10, *, mem_budget: int = 0, slots: int = 2,
-                 max_batch_queries: int = 1024, max_pending: int = 4096):
+                 max_batch_queries: int = 1024, max_pending: int = 4096,
+                 batch_cells: float = 0.0):
         if aligner._refs is None:
             raise ValueError("call index(refs) on the aligner first")
         self.aligner = aligner
@@ -55,6 +56,8 @@ class Server:
                 int(mem_budget), int(slots), int(max_batch_queries), int(max_pending),
                 ctypes.byref(h)))
         self.handle = h
+        if batch_cells:  # work per batch in cells (0: the engine default)
+            self._check(self.lib.gpusw_server_set_batch_cells(self.handle, float(batch_cells)))
 
     def _check(self, rc: int):
         if rc != _native.OK:

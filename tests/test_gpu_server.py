@@ -84,3 +84,25 @@ def test_cancel_queue_full_budget_and_timeouts():
         rid = tiny.submit(small[2])      # a small one still fits
         idx, _ = tiny.result(rid, timeout=60)
         assert idx.shape == (2, 3)
+
+
+def test_large_request_runs_in_parts_and_small_ones_share_batches():
+    """A request above one batch's work (the default 3e12 cells) is cut into parts; the parts
+    and the small requests queued behind it come back bit-identical to scoring them alone."""
+    rng, refs = _db(4, n=3000, lo=950, hi=1050)       # ~3.0e6 reference residues
+    sch = schemes.DNA
+    big = rand_seqs(rng, 1200, 900, 1000, "ACGT")       # ~3.4e12 cells
+    small = [rand_seqs(rng, int(rng.integers(1, 4)), 50, 300, "ACGT") for _ in range(5)]
+    al = Aligner(sch).index(refs)
+    want_big = al.top_k(big, k=4)
+    want_small = [al.top_k(q, k=4) for q in small]
+    with Server(Aligner(sch).index(refs), k=4, slots=1, max_batch_queries=2048) as srv:
+        ib = srv.submit(big)
+        ids = [srv.submit(q) for q in small]
+        got_small = [srv.result(i, timeout=300) for i in ids]
+        idx, sc = srv.result(ib, timeout=300)
+        st = srv.stats()
+    assert np.array_equal(idx, want_big.topk_idx) and np.array_equal(sc, want_big.topk_scores)
+    for (i2, s2), w in zip(got_small, want_small):
+        assert np.array_equal(i2, w.topk_idx) and np.array_equal(s2, w.topk_scores)
+    assert st["completed"] == 6 and st["batches"] >= 2

@@ -264,6 +264,17 @@ class Aligner:
             self._record(ctx, "sw_locate")
         return res
 
+    def locate_top(self, result: AlignResult) -> dict:
+        """Coordinates of every hit of ``result``, a ``top_k`` result for this aligner's
+        current queries: the arrays of :meth:`locate`, shaped like ``result.topk_idx``."""
+        idx = np.asarray(result.topk_idx)
+        if idx.ndim != 2 or self._queries is None or idx.shape[0] != self._queries.n:
+            raise ValueError("locate_top() takes a top_k result of this aligner's current queries")
+        nq, k = idx.shape
+        qi = np.repeat(np.arange(nq, dtype=np.int32), k)
+        loc = self.locate(qi, idx.reshape(-1).astype(np.int32))
+        return {key: v.reshape(nq, k) for key, v in loc.items()}
+
     # ----------------------------------------------------------------- introspection
     @property
     def backend(self) -> str:

@@ -1,18 +1,20 @@
 """Command-line interface over the B200 engine: score FASTA files.
 
     python -m gpusw_b200 cross --queries q.fasta --refs r.fasta --scheme dna -o scores.csv
-    python -m gpusw_b200 topk  --queries q.fasta --refs r.fasta --scheme blosum62 -k 5
+    python -m gpusw_b200 topk  --queries q.fasta --refs r.fasta --scheme blosum62 -k 5 [--coords]
     python -m gpusw_b200 pairs --queries q.fasta --refs r.fasta --scheme dna
     python -m gpusw_b200 info
 
 Same subcommands, options and CSV layouts as the reference package's CLI
 (``src/gpusw/cli.py:28-143``); the top-k subcommand streams one query block at a time to
-the CSV and reports GCUPS on stderr.
+the CSV and reports GCUPS on stderr, and with ``--coords`` adds the coordinates of each
+hit's best local alignment (the reference recovers those by re-aligning on the CPU).
 """
 from __future__ import annotations
 
 import argparse
 import csv
+import os
 import sys
 
 from . import (
@@ -75,17 +77,27 @@ def _cmd_cross(args) -> int:
 
 
 def _cmd_topk(args) -> int:
-    qs, rs = read_fasta(args.queries), read_fasta(args.refs)
+    qs = read_fasta(args.queries)
+    if not os.path.exists(args.refs):
+        raise FileNotFoundError(f"FASTA file not found: {args.refs}")
     al = Aligner(_build_scheme(**_scheme_kw(args)), threads=args.threads, backend=args.backend)
-    al.index(rs)
+    al.index(args.refs)  # the path: read and encoded by the engine library's FASTA reader
     block = max(1, args.block)
+    head = ["query", "rank", "reference", "score"]
+    if args.coords:
+        head += ["query_start", "query_end", "ref_start", "ref_end"]
     with _Out(args.out) as w:
-        w.writerow(["query", "rank", "reference", "score"])
+        w.writerow(head)
         for b0 in range(0, len(qs), block):
             res = al.top_k(qs[b0:b0 + block], k=args.k)
-            for qid, hits in res.top_k(args.k):
+            loc = al.locate_top(res) if args.coords else None
+            for qi, (qid, hits) in enumerate(res.top_k(args.k)):
                 for rank, (rid, sc) in enumerate(hits, 1):
-                    w.writerow([qid, rank, rid, sc])
+                    row = [qid, rank, rid, sc]
+                    if loc is not None:
+                        row += [int(loc[key][qi, rank - 1])
+                                for key in ("query_start", "query_end", "ref_start", "ref_end")]
+                    w.writerow(row)
     sys.stderr.write(f"[gpusw_b200] {al.gcups:.1f} GCUPS\n")
     return 0
 
@@ -126,6 +138,9 @@ def main(argv=None) -> int:
     _scoring_args(pt)
     pt.add_argument("-k", type=int, default=5)
     pt.add_argument("--block", type=int, default=4096, help="queries per streamed block")
+    pt.add_argument("--coords", action="store_true",
+                    help="add 0-based, end-exclusive coordinates of each hit's best local "
+                         "alignment (local schemes; -1 where the score is 0)")
     pt.set_defaults(func=_cmd_topk)
     pp = sub.add_parser("pairs", help="score queries vs refs 1:1")
     _scoring_args(pp)

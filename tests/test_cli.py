@@ -58,6 +58,12 @@ def test_cli_cross_topk_pairs(tmp_path):
     rows = _rows(out)
     assert rows[0] == ["query", "rank", "reference", "score"] and len(rows) == 1 + 2 * 2
     assert rows[1][0] == "qa" and rows[1][2] == "ra"
+    out = str(tmp_path / "topk_coords.csv")
+    assert main(["topk", "--queries", q, "--refs", r3, "--scheme", "dna", "-k", "2", "-o", out,
+                 "--coords"]) == 0
+    rows = _rows(out)
+    assert rows[0][4:] == ["query_start", "query_end", "ref_start", "ref_end"]
+    assert rows[1][:4] == ["qa", "1", "ra", "16"] and rows[1][4:] == ["0", "8", "0", "8"]
     q2 = _fasta(tmp_path, "q2.fasta", [("qa", "ACGT"), ("qb", "TTTT")])
     r2 = _fasta(tmp_path, "r2.fasta", [("ra", "ACGT"), ("rb", "TTTA")])
     out = str(tmp_path / "pairs.csv")

@@ -93,3 +93,19 @@ def test_locate_scores_equal_score_pairs():
     qi = rng.integers(0, 200, size=500).astype(np.int32)
     rj = rng.integers(0, 200, size=500).astype(np.int32)
     assert np.array_equal(al.locate(qi, rj)["score"], al.score_pairs(qi, rj))
+
+
+def test_locate_top_hits_match_oracle():
+    rng = np.random.default_rng(24)
+    alpha = "ARNDCQEGHILKMFPSTWYV"
+    refs = rand_seqs(rng, 120, 40, 400, alpha)
+    qs_ = [_mutate(rng, refs[int(rng.integers(0, 120))][10:200], alpha, 0.15) for _ in range(9)]
+    sch = schemes.BLOSUM62
+    al = Aligner(sch).index(refs)
+    res = al.top_k(qs_, k=3)
+    loc = al.locate_top(res)
+    assert np.array_equal(loc["score"], res.topk_scores)
+    qi = np.repeat(np.arange(9, dtype=np.int32), 3)
+    want = oracle.locate_pairs(al._queries, al._refs, qi, res.topk_idx.reshape(-1), sch)
+    for k in KEYS:
+        assert np.array_equal(loc[k].reshape(-1).astype(np.int64), want[k]), k

@@ -174,3 +174,27 @@ def test_large_alphabet_eight_bit_codes():
     got = align_score(qs, rs, scheme=scheme, return_ids=False)
     want = oracle.score_cross(funnel(qs, scheme), funnel(rs, scheme), scheme)
     assert np.array_equal(got.astype(np.int64), want)
+
+
+@pytest.mark.parametrize("scheme,alpha,hi", [
+    (Scheme(mode="local", match=100, mismatch=-60, gap_open=-50, gap_extend=-10), "ACGT", 200),
+    (Scheme(mode="semiglobal", free_end_gaps_query=True, free_end_gaps_ref=False), "ACGTN", 400),
+    (Scheme(mode="semiglobal", free_end_gaps_query=False, free_end_gaps_ref=True), "ACGTN", 400),
+    (Scheme(mode="global"), "ACGT", 400),
+    (Scheme(mode="local", matrix=Matrix.named("BLOSUM62"), gap_open=-11, gap_extend=-1),
+     "ARNDCQEGHILKMFPSTWYV", 1300),
+], ids=["profile_beyond_int8", "semi_free_query_only", "semi_free_ref_only", "global",
+        "blosum62_multipass"])
+def test_pairs_kernel_paths(scheme, alpha, hi):
+    """Every form of the pairs kernel: int8 or s16x2 query tables, the branch-free pass and
+    the general one (free query ends without left padding), one or several column passes,
+    partners of unequal row lengths."""
+    rng = np.random.default_rng(hi + len(alpha))
+    qs = rand_seqs(rng, 160, 0, hi, alpha)
+    rs = rand_seqs(rng, 160, 0, hi, alpha)
+    qi = rng.permutation(160).astype(np.int32)
+    rj = rng.integers(0, 160, size=160).astype(np.int32)
+    al = Aligner(scheme).index(rs).set_queries(qs)
+    got = al.score_pairs(qi, rj)
+    want = oracle.score_pairs(funnel(qs, scheme), funnel(rs, scheme), qi, rj, scheme)
+    assert np.array_equal(got.astype(np.int64), want)

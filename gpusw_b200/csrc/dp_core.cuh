@@ -879,15 +879,15 @@ __device__ __forceinline__ void team_stream_local(const SchemeDev& S, const uint
     cb_next = cp[t + 1];
     uint32_t e_in = __shfl_up_sync(wmask, e_out, 1, G);
     uint32_t x_in = __shfl_up_sync(wmask, x_out, 1, G);
-    if (lane == 0) {
-      if (has_prev) {
+    if (has_prev) {  // uniform across the team
+      if (lane == 0) {
         const uint2 b = bnd[t];
         e_in = b.x;
         x_in = b.y;
-      } else {
-        e_in = NEGE0;
-        x_in = GO;
       }
+    } else {  // lane 0's row-0 boundary by selection, no divergent branch
+      e_in = lane == 0 ? NEGE0 : e_in;
+      x_in = lane == 0 ? GO : x_in;
     }
     const int code = cb & 0x7F;
     const uint4* pr = prof + code * pstride + lane;

@@ -306,7 +306,8 @@ class Aligner:
             f"#define GEXT ({mf['gap_extend']})",
             f"#define FREE_Q ({int(mf['free_q'])})",
             f"#define FREE_R ({int(mf['free_r'])})",
-            "// entry points: sw_cross -> gsw::cross_kernel, sw_pairs -> gsw::pairs_kernel",
+            "// entry points: sw_cross -> gsw::cross_stream_kernel (local) or gsw::pairs_kernel"
+            " in cross mode; sw_pairs -> gsw::pairs_kernel",
             "",
         ]
         body = []

@@ -111,15 +111,14 @@ struct HostScheme {
   std::vector<int> sub;
 };
 
-// Kernel shapes compiled for the two kernels: team size G and columns per lane W.
+// Kernel shapes compiled: team size G and columns per lane W.
 struct Shape {
   int G, W;
   int cap() const { return G * W; }
 };
-const Shape kCrossShapes[] = {{8, 8}, {16, 8}, {16, 16}, {32, 16}, {32, 32}};
+// Pairs kernel shapes (explicit pairs, and the cross products of non-local schemes).
 const Shape kPairShapes[] = {{8, 8},  {8, 12},  {8, 16},  {8, 20},
                              {8, 24}, {16, 16}, {16, 24}, {32, 16}};
-constexpr int kNumCross = sizeof(kCrossShapes) / sizeof(Shape);
 // Local-mode streaming kernel shapes (columns per pass = G * W).
 const Shape kStreamShapes[] = {{8, 4},   {8, 8},   {8, 12},  {8, 16},  {8, 24},
                                {8, 32},  {16, 16}, {16, 20}, {16, 24}, {16, 32},
@@ -415,47 +414,6 @@ void require_scheme(gpusw_ctx* c, const Db& a, const Db& b) {
 }
 
 // -------------------------------------------------------------------------- launches
-template <int G, int W, int P, bool L>
-void launch_cross_t(gpusw_ctx* c, const gsw::CrossParams& prm, size_t smem) {
-  auto k = gsw::cross_kernel<G, W, P, L>;
-  static int configured_dev = -1;
-  static int blocks_per_sm = 1;
-  static size_t configured_smem = 0;
-  if (configured_dev != c->device || configured_smem < smem) {
-    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(smem, configured_smem)));
-    configured_smem = std::max(smem, configured_smem);
-    configured_dev = c->device;
-  }
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k, 256, smem));
-  int grid = c->sms * std::max(1, blocks_per_sm);
-  grid = (int)std::min<long long>(grid, std::max(1, prm.n_items));
-  k<<<grid, 256, smem, c->stream>>>(prm);
-  CK(cudaGetLastError());
-  c->st.last_launches++;
-}
-
-template <int P, bool L>
-void launch_cross_shape(gpusw_ctx* c, int shape, const gsw::CrossParams& prm, size_t smem) {
-  switch (shape) {
-    case 0: launch_cross_t<8, 8, P, L>(c, prm, smem); break;
-    case 1: launch_cross_t<16, 8, P, L>(c, prm, smem); break;
-    case 2: launch_cross_t<16, 16, P, L>(c, prm, smem); break;
-    case 3: launch_cross_t<32, 16, P, L>(c, prm, smem); break;
-    case 4: launch_cross_t<32, 32, P, L>(c, prm, smem); break;
-    default: fail(GPUSW_ERR_INVALID, "bad cross kernel shape");
-  }
-}
-
-void launch_cross(gpusw_ctx* c, int shape, int P, bool local, const gsw::CrossParams& prm, size_t smem) {
-  if (P == 2) {
-    if (local) launch_cross_shape<2, true>(c, shape, prm, smem);
-    else launch_cross_shape<2, false>(c, shape, prm, smem);
-  } else {
-    if (local) launch_cross_shape<1, true>(c, shape, prm, smem);
-    else launch_cross_shape<1, false>(c, shape, prm, smem);
-  }
-}
-
 // Teams per CTA of the pairs kernel: each team holds its own profile.
 int pair_teams(const Shape& s, int ns) {
   const int t = (int)std::min<size_t>(256 / s.G, kSmemCap / profile_bytes(s, ns));
@@ -558,12 +516,8 @@ void launch_pairs(gpusw_ctx* c, Bufs& B, int shape, int P, bool local, const gsw
   }
 }
 
-// Smallest compiled shape whose columns cover `ncols` and whose profile fits; -1 if none.
-int pick_cross_shape(int ncols, int ns) {
-  for (int i = 0; i < kNumCross; ++i)
-    if (kCrossShapes[i].cap() >= ncols && profile_bytes(kCrossShapes[i], ns) <= kSmemCap) return i;
-  return -1;
-}
+// Smallest pairs shape whose columns cover `ncols` and whose profile fits, else the widest
+// that fits (multi-pass).
 int pick_pair_shape(int ncols, int ns) {
   for (int i = 0; i < kNumPair; ++i)
     if (kPairShapes[i].cap() >= ncols && profile_bytes(kPairShapes[i], ns) <= kSmemCap) return i;
@@ -1001,101 +955,59 @@ void run_cross(gpusw_ctx* c, Bufs& B, const Db& q, const Db& r, const int32_t* q
     pair_out[i] = make_int2(a, b);
     pair_cols[i] = std::max(q.len[qlist[a]], b >= 0 ? q.len[qlist[b]] : 0);
   }
-  // bins by kernel shape; columns longer than any shape go to the multi-pass pairs kernel
-  int plain_shape = -2;
-  if (c->plain) {
-    const int mx = *std::max_element(pair_cols.begin(), pair_cols.end());
-    plain_shape = pick_cross_shape(std::max(1, mx), h.ns);
-  }
-  std::vector<std::vector<int>> bins(kNumCross);
-  std::vector<int> longp;
-  for (int i = 0; i < npairs; ++i) {
-    const int s = c->plain ? plain_shape : pick_cross_shape(std::max(1, pair_cols[i]), h.ns);
-    if (s < 0) longp.push_back(i);
-    else bins[s].push_back(i);
-  }
-  // rows: longest first (batched) or input order (plain); chunks of rows per work item
-  const int* row_perm_d = c->plain ? r.ident_d : r.perm_d;
-  const std::vector<int>* row_order = &r.perm_desc;
-  std::vector<int> ident;
-  if (c->plain) {
-    ident.resize(nr);
-    std::iota(ident.begin(), ident.end(), 0);
-    row_order = &ident;
-  }
+  // Cross products the streaming kernel does not take (global and semiglobal, or codes
+  // above 126) run on the pairs kernel in cross mode -- its branch-free pass, int8 tables
+  // and, for semiglobal with both ends free, left padding: work item = (column pair, one
+  // reference), one launch per pairs shape (the plain form: one shape for all pairs, sized
+  // to the longest, references in input order).
+  std::vector<std::vector<int>> pbins(kNumPair);
+  const int plain_shape =
+      c->plain ? pick_pair_shape(std::max(1, *std::max_element(pair_cols.begin(), pair_cols.end())), h.ns) : -1;
+  for (int i = 0; i < npairs; ++i)
+    pbins[c->plain ? plain_shape : pick_pair_shape(std::max(1, pair_cols[i]), h.ns)].push_back(i);
   Staging stg;
-  const size_t off_pairs = stg.add(pairs.data(), pairs.size() * sizeof(int2));
-  const size_t off_pout = stg.add(pair_out.data(), pair_out.size() * sizeof(int2));
-  struct Launch { int shape; size_t items_off; int n_items; int rows_per_item; };
-  std::vector<Launch> launches;
-  for (int s = 0; s < kNumCross; ++s) {
-    if (bins[s].empty()) continue;
-    const int teams = 256 / kCrossShapes[s].G;
-    const int rpi = c->plain ? teams * 2 : teams * 4;
-    const int nchunks = (nr + rpi - 1) / rpi;
-    // chunk cost: rows are sorted, so chunk order is already costliest first
-    std::vector<int2> items;
-    items.reserve((size_t)nchunks * bins[s].size());
-    for (int ch = 0; ch < nchunks; ++ch)
-      for (int pi : bins[s]) items.push_back(make_int2(pi, ch));
-    launches.push_back({s, stg.add(items.data(), items.size() * sizeof(int2)), (int)items.size(), rpi});
-  }
-  std::vector<int2> long_pairs, long_pout;
-  size_t off_lp = 0, off_lpo = 0;
-  for (int i : longp) { long_pairs.push_back(pairs[i]); long_pout.push_back(pair_out[i]); }
-  if (!longp.empty()) {
-    off_lp = stg.add(long_pairs.data(), long_pairs.size() * sizeof(int2));
-    off_lpo = stg.add(long_pout.data(), long_pout.size() * sizeof(int2));
+  struct PL { int shape; size_t off_p, off_o; int n; int mcol; };
+  std::vector<PL> pl;
+  for (int sh = 0; sh < kNumPair; ++sh) {
+    if (pbins[sh].empty()) continue;
+    std::vector<int2> bp, bo;
+    int mcol = 0;
+    for (int i : pbins[sh]) {
+      bp.push_back(pairs[i]);
+      bo.push_back(pair_out[i]);
+      mcol = std::max(mcol, pair_cols[i]);
+    }
+    const size_t op = stg.add(bp.data(), bp.size() * sizeof(int2));
+    const size_t oo = stg.add(bo.data(), bo.size() * sizeof(int2));
+    pl.push_back({sh, op, oo, (int)bp.size(), mcol});
   }
   char* dmeta = stg.upload(c, B);
-  const int nq_slots = (int)launches.size() + 2;
-  unsigned long long* queues = B.queue.as<unsigned long long>(nq_slots);
-  CK(cudaMemsetAsync(queues, 0, nq_slots * sizeof(unsigned long long), c->stream));
+  const int nslots = (int)pl.size() + 2;
+  unsigned long long* queues = B.queue.as<unsigned long long>(nslots);
+  CK(cudaMemsetAsync(queues, 0, nslots * sizeof(unsigned long long), c->stream));
   if (P == 2) CK(cudaMemsetAsync(B.ovf_count.as<int>(1), 0, sizeof(int), c->stream));
-  gsw::CrossParams cp{};
-  cp.S = make_scheme(h, P);
-  cp.sub = c->sub_d;
-  cp.cols = q.packed();
-  cp.rows = r.packed();
-  cp.pairs = reinterpret_cast<const int2*>(dmeta + off_pairs);
-  cp.pair_out = reinterpret_cast<const int2*>(dmeta + off_pout);
-  cp.row_perm = row_perm_d;
-  cp.n_rows = nr;
-  cp.out = out;
-  cp.out_ld = out_ld;
-  cp.ovf = B.ovf.as<gsw::Ovf>(kOvfCap);
-  cp.ovf_count = B.ovf_count.as<int>(1);
-  cp.ovf_cap = kOvfCap;
+  gsw::PairsParams pp{};
+  pp.S = make_scheme(h, P);
+  pp.sub = c->sub_d;
+  pp.cols = q.packed();
+  pp.rows = r.packed();
+  pp.item_mode = 2;
+  pp.row_perm = c->plain ? r.ident_d : r.perm_d;
+  pp.n_rows = nr;
+  pp.out_ld = out_ld;
+  pp.out = out;
+  pp.ovf = B.ovf.as<gsw::Ovf>(kOvfCap);
+  pp.ovf_count = B.ovf_count.as<int>(1);
+  pp.ovf_cap = kOvfCap;
   int slot = 0;
-  for (const Launch& L : launches) {
-    cp.items = reinterpret_cast<const int2*>(dmeta + L.items_off);
-    cp.n_items = L.n_items;
-    cp.rows_per_item = L.rows_per_item;
-    cp.queue = reinterpret_cast<int*>(queues + slot++);
-    launch_cross(c, L.shape, P, local, cp, profile_bytes(kCrossShapes[L.shape], h.ns));
-  }
-  if (!longp.empty()) {
-    gsw::PairsParams pp{};
-    pp.S = cp.S;
-    pp.sub = c->sub_d;
-    pp.cols = cp.cols;
-    pp.rows = cp.rows;
-    pp.item_mode = 2;
-    pp.pairs = reinterpret_cast<const int2*>(dmeta + off_lp);
-    pp.pair_out = reinterpret_cast<const int2*>(dmeta + off_lpo);
-    pp.row_perm = r.perm_d;
-    pp.n_rows = nr;
-    pp.out_ld = out_ld;
-    pp.n_items = (long long)longp.size() * nr;
+  for (const PL& L : pl) {
+    pp.pairs = reinterpret_cast<const int2*>(dmeta + L.off_p);
+    pp.pair_out = reinterpret_cast<const int2*>(dmeta + L.off_o);
+    pp.n_items = (long long)L.n * nr;
     pp.queue = queues + slot++;
-    pp.out = out;
-    pp.ovf = cp.ovf;
-    pp.ovf_count = cp.ovf_count;
-    pp.ovf_cap = kOvfCap;
-    launch_pairs(c, B, pick_pair_shape(1 << 30, h.ns), P, local, pp, r.max_len, true);
+    launch_pairs(c, B, L.shape, P, local, pp, r.max_len, L.mcol > kPairShapes[L.shape].cap());
   }
   if (P == 2) launch_overflow_rescore(c, B, q, r, out, queues + slot++);
-  (void)row_order;
 }
 
 // Largest number of int16 cells flagged by any one launch sequence of the call (read after

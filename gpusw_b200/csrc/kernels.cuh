@@ -69,83 +69,6 @@ __device__ __forceinline__ Acc reduce_acc(const SchemeDev& S, Acc a, unsigned wm
 }
 
 // -------------------------------------------------------------------------------------
-// Cross product: work item = (column pair, chunk of `rows_per_item` rows). The CTA builds
-// the pair's profile once and its teams walk the chunk's rows.
-struct CrossParams {
-  SchemeDev S;
-  const int* sub;
-  Packed cols, rows;
-  const int2* pairs;       // column sequences of each pair (c1 = -1: none)
-  const int2* pair_out;    // output row of each half in `out`
-  const int* row_perm;     // row sequences, longest first
-  int n_rows, rows_per_item;
-  const int2* items;       // (pair, chunk), costliest first
-  int n_items;
-  int* queue;              // work counter, zero at launch
-  int* out;                // int32 scores, out[out_row * out_ld + row_seq]
-  long long out_ld;
-  Ovf* ovf;
-  int* ovf_count;
-  int ovf_cap;
-};
-
-template <int G, int W, int P, bool LOCAL>
-__global__ void __launch_bounds__(256) cross_kernel(const CrossParams p) {
-  extern __shared__ uint4 smem_prof[];
-  __shared__ int s_item;
-  constexpr int SLOTS = G * W / 4;
-  const int pstride = (SLOTS + 7) & ~7;
-  const int team = threadIdx.x / G, lane = threadIdx.x % G, nteams = blockDim.x / G;
-  const unsigned wmask = (G == 32) ? 0xFFFFFFFFu
-                                   : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
-  for (;;) {
-    if (threadIdx.x == 0) s_item = atomicAdd(p.queue, 1);
-    __syncthreads();
-    const int it = s_item;
-    __syncthreads();
-    if (it >= p.n_items) break;
-    const int2 item = p.items[it];
-    const int2 pr = p.pairs[item.x], po = p.pair_out[item.x];
-    const int n0 = pr.x >= 0 ? p.cols.len[pr.x] : 0;
-    const int n1 = (P == 2 && pr.y >= 0) ? p.cols.len[pr.y] : 0;
-    build_profile<G, W, P>(p.S, p.sub, p.cols, pr.x, n0, P == 2 ? pr.y : -1, n1, 0, smem_prof,
-                           pstride, threadIdx.x, blockDim.x);
-    __syncthreads();
-    const int r_begin = item.y * p.rows_per_item;
-    const int r_end = min(p.n_rows, r_begin + p.rows_per_item);
-    for (int rr = r_begin + team; rr < r_end; rr += nteams) {
-      const int rs = p.row_perm[rr];
-      const int m = p.rows.len[rs];
-      Acc acc = init_acc<P>(p.S);
-      if (m > 0 && max(n0, n1) > 0) {
-        team_pass<G, W, P, LOCAL, false>(p.S, smem_prof, pstride, p.rows.words + p.rows.woff[rs],
-                                         nullptr, p.rows.bits, p.rows.per, m, m, n0, n1, 0,
-                                         nullptr, false, false, lane, wmask, acc);
-        acc = reduce_acc<G, P>(p.S, acc, wmask);
-      }
-      if (lane == 0) {
-#pragma unroll
-        for (int h = 0; h < P; ++h) {
-          const int c = h ? pr.y : pr.x;
-          if (c < 0) continue;
-          const int nh = h ? n1 : n0;
-          const long long pos = (long long)(h ? po.y : po.x) * p.out_ld + rs;
-          bool ovf = false;
-          int score = (m == 0 || nh == 0) ? empty_score(p.S, nh, m)
-                                           : finish_score<P>(p.S, acc, h, &ovf);
-          if (P == 2 && ovf && m > 0 && nh > 0) {
-            push_overflow(p.ovf, p.ovf_count, p.ovf_cap, c, rs, pos);
-            score = INT_MIN;
-          }
-          p.out[pos] = score;
-        }
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// -------------------------------------------------------------------------------------
 // Pairs: work item = P alignments (one per register half), each with its own column and
 // row sequence. The team builds its own profile for every column pass; passes hand the
 // boundary column over through a per-team scratch strip in global memory.

@@ -120,9 +120,12 @@ struct Shape {
 const Shape kPairShapes[] = {{8, 8},  {8, 12},  {8, 16},  {8, 20},
                              {8, 24}, {16, 16}, {16, 24}, {32, 16}};
 // Local-mode streaming kernel shapes (columns per pass = G * W).
+// The last four fill the 160 / 224 / 448 / 896-column gaps of the first fourteen (for
+// uneven lengths the planner otherwise pads a query up to the next cap).
 const Shape kStreamShapes[] = {{8, 4},   {8, 8},   {8, 12},  {8, 16},  {8, 24},
                                {8, 32},  {16, 16}, {16, 20}, {16, 24}, {16, 32},
-                               {32, 16}, {32, 20}, {32, 24}, {32, 32}};
+                               {32, 16}, {32, 20}, {32, 24}, {32, 32}, {8, 20},
+                               {8, 28},  {16, 28}, {32, 28}};
 constexpr int kNumStream = sizeof(kStreamShapes) / sizeof(Shape);
 constexpr int kNumPair = sizeof(kPairShapes) / sizeof(Shape);
 constexpr size_t kSmemCap = 200 * 1024;
@@ -713,6 +716,10 @@ void launch_stream_shape(gpusw_ctx* c, Bufs& B, int shape, const gsw::StreamPara
     case 11: launch_stream_t<32, 20, P>(c, B, prm, mt, mp); break;
     case 12: launch_stream_t<32, 24, P>(c, B, prm, mt, mp); break;
     case 13: launch_stream_t<32, 32, P>(c, B, prm, mt, mp); break;
+    case 14: launch_stream_t<8, 20, P>(c, B, prm, mt, mp); break;
+    case 15: launch_stream_t<8, 28, P>(c, B, prm, mt, mp); break;
+    case 16: launch_stream_t<16, 28, P>(c, B, prm, mt, mp); break;
+    case 17: launch_stream_t<32, 28, P>(c, B, prm, mt, mp); break;
     default: fail(GPUSW_ERR_INVALID, "bad stream kernel shape");
   }
 }
@@ -1254,7 +1261,7 @@ __global__ void dpx_rate_kernel(const unsigned* in, unsigned* out, int iters) {
 // ================================================================================ C ABI
 extern "C" {
 
-int gpusw_version(void) { return 100; }
+int gpusw_version(void) { return 101; }
 
 int gpusw_device_count(int* count) {
   if (!count) return GPUSW_ERR_INVALID;

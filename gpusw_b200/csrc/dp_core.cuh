@@ -103,6 +103,21 @@ __device__ __forceinline__ int empty_score(const SchemeDev& S, int n, int m) {
 
 // Packed residue codes: sequence words start 16-byte aligned; code c of a sequence sits
 // in word c / per at bit (c % per) * bits.
+// Code r of a packed sequence starting at word pointer w (per codes per word): shifts for
+// per = 4, 8, 16 and a multiply-high for per = 6 instead of an integer division.
+__device__ __forceinline__ uint32_t packed_row_code(const uint32_t* w, int r, int bits, int per) {
+  unsigned q, rem;
+  if (per == 6) {
+    q = __umulhi((unsigned)r, 0xAAAAAAABu) >> 2;  // r / 6 for every 32-bit r
+    rem = (unsigned)r - q * 6u;
+  } else {
+    const int sh = __ffs(per) - 1;                 // per = 4, 8 or 16
+    q = (unsigned)r >> sh;
+    rem = (unsigned)r & (unsigned)(per - 1);
+  }
+  return (__ldg(w + q) >> (rem * (unsigned)bits)) & ((1u << bits) - 1u);
+}
+
 struct Packed {
   const uint32_t* words;
   const long long* woff;  // first word of each sequence
@@ -111,6 +126,11 @@ struct Packed {
   __device__ __forceinline__ int code(int seq, int c) const {
     uint32_t w = __ldg(words + woff[seq] + c / per);
     return (int)((w >> ((c % per) * bits)) & ((1u << bits) - 1u));
+  }
+  // The same code without an integer division (the per-team profile builders of the pairs
+  // kernel, where the decode is a visible share of a short alignment's work).
+  __device__ __forceinline__ int code_fast(int seq, int c) const {
+    return (int)packed_row_code(words + woff[seq], c, bits, per);
   }
 };
 
@@ -123,6 +143,10 @@ struct ByteSeqs {
   __device__ __forceinline__ int length(int s) const { return off[s + 1] - off[s]; }
   __device__ __forceinline__ int code(int s, int c) const { return (int)__ldg(codes + off[s] + c); }
 };
+
+// Residue code for the per-team profile builders: packed sets decode without a division.
+__device__ __forceinline__ int seq_code(const Packed& s, int seq, int c) { return s.code_fast(seq, c); }
+__device__ __forceinline__ int seq_code(const ByteSeqs& s, int seq, int c) { return s.code(seq, c); }
 
 // Lane 0's code feed for a byte-coded row: the team_pass call passes the row's first
 // byte through its word-pointer parameter; one byte per step, the pad code past the end.
@@ -406,7 +430,7 @@ __device__ __forceinline__ void build_profile_lane(const SchemeDev& S, const int
 #pragma unroll
     for (int k = 0; k < W; ++k) {
       const int j = col0 + lane * W + k - pd;  // real column, or < 0 (dummy) / >= n (past end)
-      code[h][k] = (c >= 0 && j >= 0 && j < n) ? cols.code(c, j) : (j < 0 ? -1 : -2);
+      code[h][k] = (c >= 0 && j >= 0 && j < n) ? seq_code(cols, c, j) : (j < 0 ? -1 : -2);
     }
   }
   for (int a = 0; a <= S.ns; ++a) {
@@ -448,7 +472,7 @@ __device__ __forceinline__ void build_profile_lane8(const SchemeDev& S, const in
 #pragma unroll
     for (int k = 0; k < W; ++k) {
       const int j = col0 + lane * W + k - pd;  // real column, or < 0 (dummy) / >= n (past end)
-      code[k] = (c >= 0 && j >= 0 && j < n) ? cols.code(c, j) : (j < 0 ? -1 : -2);
+      code[k] = (c >= 0 && j >= 0 && j < n) ? seq_code(cols, c, j) : (j < 0 ? -1 : -2);
     }
     for (int a = 0; a <= S.ns; ++a) {
       uint32_t* row = prof + a * pstride8 + lane;
@@ -522,20 +546,6 @@ __device__ __forceinline__ void team_argmax(Acc& a, unsigned wmask) {
 // Not covered (team_pass is used instead): LOCATE, and the non-left-padded semiglobal mode
 // with free query ends, whose end column needs a mask per cell.
 constexpr int kRing = 128, kRingHalf = kRing / 2;
-
-// Code of row r of a packed sequence starting at word pointer w (per codes per word).
-__device__ __forceinline__ uint32_t packed_row_code(const uint32_t* w, int r, int bits, int per) {
-  unsigned q, rem;
-  if (per == 6) {
-    q = __umulhi((unsigned)r, 0xAAAAAAABu) >> 2;  // r / 6 for every 32-bit r
-    rem = (unsigned)r - q * 6u;
-  } else {
-    const int sh = __ffs(per) - 1;                 // per = 4, 8 or 16
-    q = (unsigned)r >> sh;
-    rem = (unsigned)r & (unsigned)(per - 1);
-  }
-  return (__ldg(w + q) >> (rem * (unsigned)bits)) & ((1u << bits) - 1u);
-}
 
 template <int G, int W, int P, bool LOCAL, bool LEFTPAD, bool P8>
 struct FastPass {

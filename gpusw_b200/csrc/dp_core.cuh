@@ -456,37 +456,41 @@ __device__ __forceinline__ void build_profile_lane(const SchemeDev& S, const int
 
 // Int8 form of build_profile_lane for two halves (P = 2, used when every profile value fits
 // in a signed byte): half h's values go to its own table profH, four columns per 32-bit
-// slot k4 * G + lane of each code row (pstride8 slots per row). Values as above.
+// slot k4 * G + lane of each code row (pstride8 slots per row). The values come from `ext`,
+// the per-block table of every (column class, row code) byte (see pairs_ext_stride): for
+// each group of four columns and four row codes, four 32-bit loads and a 4 x 4 byte
+// transpose (eight byte permutes) give the four row words.
 template <int G, int W, class Seqs = Packed>
-__device__ __forceinline__ void build_profile_lane8(const SchemeDev& S, const int* sub,
+__device__ __forceinline__ void build_profile_lane8(const SchemeDev& S, const uint32_t* ext,
                                                     const Seqs& cols, int c0, int n0, int pad0,
                                                     int c1, int n1, int pad1, int col0,
                                                     uint32_t* prof0, uint32_t* prof1,
                                                     int pstride8, int lane) {
-  const int pad_s = S.s_pad - S.go, zero_s = -S.go;
+  const int rw = ((S.ns + 1 + 3) & ~3) / 4;  // 32-bit words per column class
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const int c = h ? c1 : c0, n = h ? n1 : n0, pd = h ? pad1 : pad0;
     uint32_t* prof = h ? prof1 : prof0;
-    int code[W];
+    int cls[W];
 #pragma unroll
     for (int k = 0; k < W; ++k) {
       const int j = col0 + lane * W + k - pd;  // real column, or < 0 (dummy) / >= n (past end)
-      code[k] = (c >= 0 && j >= 0 && j < n) ? seq_code(cols, c, j) : (j < 0 ? -1 : -2);
+      cls[k] = (c >= 0 && j >= 0 && j < n) ? seq_code(cols, c, j) : (j < 0 ? S.ns : S.ns + 1);
+      cls[k] *= rw;
     }
-    for (int a = 0; a <= S.ns; ++a) {
-      uint32_t* row = prof + a * pstride8 + lane;
+    for (int rg = 0; rg < rw; ++rg) {
+      uint32_t* row = prof + (4 * rg) * pstride8 + lane;
 #pragma unroll
-      for (int k4 = 0; k4 < W / 4; ++k4) {
-        uint32_t v = 0;
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int cd = code[4 * k4 + e];
-          const int hv = cd >= 0 ? (a < S.ns ? sub[a * S.ns + cd] - S.go : pad_s)
-                                 : (cd == -1 ? (a < S.ns ? zero_s : pad_s) : pad_s);
-          v |= (uint32_t)(hv & 0xFF) << (8 * e);
-        }
-        row[k4 * G] = v;
+      for (int g = 0; g < W / 4; ++g) {
+        const uint32_t w0 = ext[cls[4 * g] + rg], w1 = ext[cls[4 * g + 1] + rg];
+        const uint32_t w2 = ext[cls[4 * g + 2] + rg], w3 = ext[cls[4 * g + 3] + rg];
+        const uint32_t t0 = __byte_perm(w0, w1, 0x5140), t1 = __byte_perm(w0, w1, 0x7362);
+        const uint32_t t2 = __byte_perm(w2, w3, 0x5140), t3 = __byte_perm(w2, w3, 0x7362);
+        // row 4 rg + r, columns 4 g .. 4 g + 3
+        row[g * G] = __byte_perm(t0, t2, 0x5410);
+        if (4 * rg + 1 <= S.ns) row[pstride8 + g * G] = __byte_perm(t0, t2, 0x7632);
+        if (4 * rg + 2 <= S.ns) row[2 * pstride8 + g * G] = __byte_perm(t1, t3, 0x5410);
+        if (4 * rg + 3 <= S.ns) row[3 * pstride8 + g * G] = __byte_perm(t1, t3, 0x7632);
       }
     }
   }

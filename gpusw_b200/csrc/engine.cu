@@ -427,7 +427,7 @@ template <int G, int W, int P, bool L, bool LP, bool LOC = false, bool P8 = fals
 void launch_pairs_t(gpusw_ctx* c, Bufs& B, gsw::PairsParams prm, int /*teams_hint*/, long long max_rows, bool multipass) {
   auto k = gsw::pairs_kernel<G, W, P, L, LP, LOC, P8>;
   const Shape s{G, W};
-  const size_t sub_bytes = (size_t)gsw::pairs_sub_uint4(prm.S.ns) * 16;
+  const size_t sub_bytes = (size_t)(gsw::pairs_sub_uint4(prm.S.ns) + (P8 ? gsw::pairs_ext_uint4(prm.S.ns) : 0)) * 16;
   // per team: the profile (s16x2, or two int8 tables of one byte per column) + row-code ring
   const size_t prof = (P8 ? profile_bytes(s, prm.S.ns) / 2 : profile_bytes(s, prm.S.ns)) +
                       gsw::kRing * sizeof(uint32_t);

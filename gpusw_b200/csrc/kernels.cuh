@@ -160,6 +160,16 @@ __host__ __device__ __forceinline__ int pairs_sub_uint4(int ns) {
   return ns <= kSubSmemMax ? (ns * ns + 3) / 4 : 0;
 }
 
+// P8: after the substitution table, the int8 profile value of every (column class, row
+// code) -- classes 0..ns-1 are residue codes, ns a dummy column left of a left-padded
+// sequence, ns+1 a column past a sequence's end -- as `pairs_ext_stride(ns)` bytes per class
+// (the ns + 1 row codes, padded to whole 32-bit words), so that a lane fetches four row
+// values of a column with one 32-bit load.
+__host__ __device__ __forceinline__ int pairs_ext_stride(int ns) { return (ns + 1 + 3) & ~3; }
+__host__ __device__ __forceinline__ int pairs_ext_uint4(int ns) {
+  return ((ns + 2) * pairs_ext_stride(ns) + 15) / 16;
+}
+
 // At most 256 threads per block; one resident block is enough for the register budget, so
 // the compiler keeps every W-column state in registers (no spills in any instantiation).
 //
@@ -176,16 +186,29 @@ __global__ void __launch_bounds__(256, P8 ? 2 : 1) pairs_kernel(const PairsParam
                                    : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
   const int ns = p.S.ns;
   const int sub_u4 = pairs_sub_uint4(ns);
+  const int ext_u4 = P8 ? pairs_ext_uint4(ns) : 0;
   const int* sub = p.sub;
   if (sub_u4 > 0) {
     int* s_sub = reinterpret_cast<int*>(smem_prof);
     for (int i = threadIdx.x; i < ns * ns; i += blockDim.x) s_sub[i] = p.sub[i];
-    __syncthreads();
     sub = s_sub;
   }
+  const uint32_t* ext = reinterpret_cast<const uint32_t*>(smem_prof + sub_u4);
+  if (P8) {
+    uint8_t* e8 = reinterpret_cast<uint8_t*>(smem_prof + sub_u4);
+    const int stride = pairs_ext_stride(ns), pad_s = p.S.s_pad - p.S.go, zero_s = -p.S.go;
+    for (int i = threadIdx.x; i < (ns + 2) * stride; i += blockDim.x) {
+      const int cls = i / stride, a = i % stride;
+      int v = pad_s;
+      if (a < ns && cls < ns) v = p.sub[a * ns + cls] - p.S.go;
+      else if (a < ns && cls == ns) v = zero_s;
+      e8[i] = (uint8_t)(v & 0xFF);
+    }
+  }
+  if (sub_u4 > 0 || P8) __syncthreads();
   // per team: its profile (s16x2 table, or the two int8 tables), then its row-code ring
   const size_t team_u4 = (P8 ? (size_t)(ns + 1) * pstride / 2 : (size_t)(ns + 1) * pstride) + kRing / 4;
-  uint4* prof = smem_prof + sub_u4 + (size_t)team * team_u4;
+  uint4* prof = smem_prof + sub_u4 + ext_u4 + (size_t)team * team_u4;
   uint32_t* prof8 = reinterpret_cast<uint32_t*>(prof);
   uint32_t* ring = reinterpret_cast<uint32_t*>(prof + team_u4 - kRing / 4);
   uint2* bnd = p.bnd ? p.bnd + ((size_t)blockIdx.x * nteams + team) * p.bnd_cap : nullptr;
@@ -220,7 +243,7 @@ __global__ void __launch_bounds__(256, P8 ? 2 : 1) pairs_kernel(const PairsParam
       const uint32_t* w1 = (P == 2 && it.r[P - 1] >= 0) ? p.rows.words + p.rows.woff[it.r[P - 1]] : w0;
       for (int ps = 0; ps < npass; ++ps) {
         if constexpr (P8) {
-          build_profile_lane8<G, W>(p.S, sub, p.cols, it.valid[0] ? it.q[0] : -1, n0, pad0,
+          build_profile_lane8<G, W>(p.S, ext, p.cols, it.valid[0] ? it.q[0] : -1, n0, pad0,
                                     it.valid[P - 1] ? it.q[P - 1] : -1, n1, pad1, ps * G * W,
                                     prof8, prof8 + (ns + 1) * pstride, pstride, lane);
           team_pass_fast<G, W, P, LOCAL, LEFTPAD, true>(p.S, prof, prof8, pstride, ring, w0, w1,

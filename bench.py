@@ -330,6 +330,34 @@ def serving_sweep(aligner, loads, n_requests, seed=4, slots=2, k=10, batch_cells
     return out
 
 
+def plain_over_requests(aligner, n_requests, seed=4, k=10):
+    """The plain form over the same request stream as `serving_sweep`: every request's top-k
+    computed by itself, one request after another, with the engine's plain form (16-query
+    batches in input order, one kernel shape per batch sized to its longest query, no
+    binning, no graph). Device GCUPS (CUDA events around each call)."""
+    from gpusw_b200 import workloads
+
+    reqs = workloads.requests(seed=seed, n_requests=n_requests)
+    ctx = aligner._ctx()
+    ref_res = float(np.diff(aligner._refs.offsets).sum())
+    cells = ms = 0.0
+    with ctx.lock:
+        ctx.set_scheme(aligner.scheme)
+        ctx.set_options(plain=True)
+        try:
+            for codes, offs in reqs:
+                nq = offs.shape[0] - 1
+                q = ctx.upload(codes, offs)
+                ctx.topk(q, aligner._dref.handle, np.arange(nq, dtype=np.int32), aligner._refs.n, k,
+                         aligner._policy())
+                ms += ctx.stats().last_kernel_ms
+                cells += float(np.diff(offs).sum()) * ref_res
+                ctx.free(q)
+        finally:
+            ctx.set_options(plain=False)
+    return cells / (ms * 1e-3) / 1e9
+
+
 def run_serving(args, rank, world, local):
     """--workload serving: the serving sweep alone (16S reference set resident)."""
     from gpusw_b200 import Aligner
@@ -342,6 +370,7 @@ def run_serving(args, rank, world, local):
     loads = [float(x) for x in args.serve_loads.split(",")]
     sweep = serving_sweep(al, loads, args.serve_requests, slots=args.serve_slots,
                           batch_cells=args.serve_batch_cells)
+    plain = plain_over_requests(al, args.serve_requests)
     if rank == 0:
         top = max(sweep, key=lambda r: r["gcups"])
         print(json.dumps({"metric": METRIC, "value": top["gcups"], "unit": "GCUPS", "n_gpus": world,
@@ -353,6 +382,11 @@ def run_serving(args, rank, world, local):
                                      "slots": args.serve_slots,
                                      "batch_cells": args.serve_batch_cells or "engine default",
                                      "request_queries": "1-512 log-uniform, lengths U[50,2000]"},
+                          "plain": {"value": plain, "unit": "GCUPS",
+                                    "form": "the same requests one at a time, engine plain form "
+                                            "(16-query batches, one shape per batch sized to its "
+                                            "longest query, no binning, no graph); device time"},
+                          "served_over_plain": top["gcups"] / plain if plain > 0 else None,
                           "serving": sweep}), flush=True)
 
 

@@ -253,9 +253,16 @@ void server_loop(gpusw_server* s) {
       int nq = 0, max_len = 0;
       double cells = 0;
       std::vector<Slot::Part> take;
-      // with company in the queue no request takes more than half a batch
-      const double share = s->pending.size() > 1 ? s->batch_cells / 2 : s->batch_cells;
-      for (size_t qi = 0; qi < s->pending.size() && nq < s->max_batch && cells < s->batch_cells;) {
+      // The batch grows with the backlog: at least batch_cells, and an equal share of the
+      // queued work per slot when more is waiting (bigger batches keep the device fuller
+      // when requests queue anyway; a short queue keeps batches, and latency, small). With
+      // company in the queue no request takes more than half a batch.
+      double backlog = 0;
+      for (const SrvRequest* r : s->pending)
+        backlog += (double)(r->offsets[r->nq] - r->offsets[r->next_q]) * s->ref_residues;
+      const double target = std::max(s->batch_cells, backlog / (double)s->slots.size());
+      const double share = s->pending.size() > 1 ? target / 2 : target;
+      for (size_t qi = 0; qi < s->pending.size() && nq < s->max_batch && cells < target;) {
         SrvRequest* r = s->pending[qi];
         Slot::Part pt{r, r->next_q, 0, nq};
         double rcells = 0;
@@ -266,7 +273,7 @@ void server_loop(gpusw_server* s) {
           const double qc = (double)len * s->ref_residues;
           const int64_t qb = request_bytes(s, 1, len);
           const bool first = take.empty() && pt.nq == 0;
-          if (!first && (rcells + qc > share || cells + qc > s->batch_cells)) break;
+          if (!first && (rcells + qc > share || cells + qc > target)) break;
           if (s->in_use + bytes + rbytes + qb > s->budget) break;
           rcells += qc;
           rbytes += qb;

@@ -277,11 +277,13 @@ const char *gpusw_server_last_error(const gpusw_server *srv);
 
 /* Stop the scheduler (waiting at most for the in-flight batches) and free the server. */
 void gpusw_server_destroy(gpusw_server *srv);
-/* Work per batch in DP cells (0: the default, 3e12, about half a second on one B200).
- * Batches are cut by work, not by request: a request above it runs as several parts, and
- * while others wait no request takes more than half of a batch, so small requests queued
- * behind a large one share the next batch. Smaller values lower latency, larger ones raise
- * throughput. No reference counterpart (the reference has no server). */
+/* Least work per batch in DP cells (0: the default, 3e12, about half a second on one B200).
+ * Batches are cut by work, not by request: a batch takes this much, or an equal share per
+ * slot of all the queued work when that is larger; a request above it runs as several
+ * parts, and while others wait no request takes more than half of a batch, so small
+ * requests queued behind a large one share the next batch. Smaller values lower latency at
+ * light load; under a backlog batches grow anyway. No reference counterpart (the reference
+ * has no server). */
 int gpusw_server_set_batch_cells(gpusw_server *srv, double cells);
 
 /* ------------------------------------------------------------------ FASTA (host only)

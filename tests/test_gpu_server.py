@@ -87,8 +87,9 @@ def test_cancel_queue_full_budget_and_timeouts():
 
 
 def test_large_request_runs_in_parts_and_small_ones_share_batches():
-    """A request above one batch's work (the default 3e12 cells) is cut into parts; the parts
-    and the small requests queued behind it come back bit-identical to scoring them alone."""
+    """A request above one batch's work is cut into parts (here 1e12 cells per batch, or the
+    backlog's share per slot when larger); the parts and the small requests queued behind it
+    come back bit-identical to scoring them alone."""
     rng, refs = _db(4, n=3000, lo=950, hi=1050)       # ~3.0e6 reference residues
     sch = schemes.DNA
     big = rand_seqs(rng, 1200, 900, 1000, "ACGT")       # ~3.4e12 cells
@@ -96,7 +97,8 @@ def test_large_request_runs_in_parts_and_small_ones_share_batches():
     al = Aligner(sch).index(refs)
     want_big = al.top_k(big, k=4)
     want_small = [al.top_k(q, k=4) for q in small]
-    with Server(Aligner(sch).index(refs), k=4, slots=1, max_batch_queries=2048) as srv:
+    with Server(Aligner(sch).index(refs), k=4, slots=2, max_batch_queries=2048,
+                batch_cells=1e12) as srv:
         ib = srv.submit(big)
         ids = [srv.submit(q) for q in small]
         got_small = [srv.result(i, timeout=300) for i in ids]

@@ -528,6 +528,16 @@ def run_ours(args, rank, world, local):
         bitexact = {"pairs_checked": int(np.asarray(want).size),
                     "equal": bool(np.array_equal(np.asarray(got, dtype=np.int64), want))}
 
+    # DRAM bytes of the dominant kernel's launch, from an ncu capture: the pairs kernel reads
+    # each pair's packed codes once (14.89 MB for 100,000 read/window pairs, nothing written
+    # to DRAM), so it scales with the pairs. The streaming kernel's working set (packed
+    # references, stream bytes) is L2-resident and reused by every query pair, so a small
+    # capture (6.1 MB read for 1.9e11 cells) does not scale and is not extrapolated.
+    traffic, traffic_src = None, "not extrapolated: L2-resident working set (see profiles/)"
+    if wl.pairs is not None:
+        traffic = 14.89e6 / 1e5 * wl.pairs[0].shape[0]
+        traffic_src = "ncu dram__bytes_read+write for 100,000 pairs, scaled by the pairs"
+
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world,
                "steps": args.steps, "warmup": args.warmup,
@@ -537,7 +547,8 @@ def run_ours(args, rank, world, local):
                "data": "synthetic", "config": config_of(wl), "gpu_launches": launches,
                "roofline": {"bound": "int", "achieved": kern_gcups, "peak": peak_gcups,
                             "unit": "GCUPS", "frac": kern_gcups / peak_gcups,
-                            "traffic": None,
+                            "traffic": traffic,
+                            "traffic_source": traffic_src,
                             "peak_source": f"measured s16x2 add-max rate {dpx / 1e12:.2f} Tops/s x 2 cells"
                                            f" / {OPS_PER_CELL_PAIR} ops (live, this GPU)",
                             "kernel_ms_per_step": sum(score_ms) / args.steps,

@@ -2047,7 +2047,7 @@ constexpr size_t kNoAllocSubOff = 256;
 constexpr size_t kNoAllocStripOff = kNoAllocSubOff + 64 * 64 * 4;
 constexpr int kNoAllocMaxDevices = 64;
 
-__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 std::mutex g_noalloc_mu;
 void* g_noalloc_ptr[kNoAllocMaxDevices] = {};

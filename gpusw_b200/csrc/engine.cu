@@ -70,11 +70,33 @@ struct DevBuf {
   }
 };
 
+// Allocator whose resize() leaves elements uninitialised, so the pages of a large host
+// array are first touched by the threaded loop that fills it rather than by one thread
+// zeroing it (for 10^6 sequences that zeroing alone took 1-2 ms per set upload).
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = NoInitAlloc<U>;
+  };
+  NoInitAlloc() = default;
+  template <class U>
+  NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+  template <class U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <class U, class... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+  }
+};
+
 struct Db {
   int n = 0;
   int bits = 2, per = 16, max_code = 0, max_len = 0;
-  std::vector<int> len;
-  std::vector<long long> woff;
+  std::vector<int, NoInitAlloc<int>> len;         // filled by threaded loops in db_upload
+  std::vector<long long, NoInitAlloc<long long>> woff;
   std::vector<int> perm_desc;  // sequences by length, longest first (stable)
   void* base = nullptr;        // one allocation: words, then woff_d, then len_d
   uint32_t* words = nullptr;
@@ -1470,8 +1492,10 @@ int gpusw_db_upload(gpusw_ctx* c, const uint8_t* codes, const int32_t* offsets, 
     parallel_ranges(n, [&](long long lo, long long hi) { pack_range(codes, offsets, *d, c->pinned, (int)lo, (int)hi); });
     std::fill(c->pinned + w, c->pinned + nwords, 0u);
     if (n) {
-      memcpy(img + woff_o, d->woff.data(), (size_t)n * 8);
-      memcpy(img + len_o, d->len.data(), (size_t)n * 4);
+      parallel_ranges(n, [&](long long lo, long long hi) {
+        memcpy(img + woff_o + (size_t)lo * 8, d->woff.data() + lo, (size_t)(hi - lo) * 8);
+        memcpy(img + len_o + (size_t)lo * 4, d->len.data() + lo, (size_t)(hi - lo) * 4);
+      });
     }
     tr.lap("pack");
     CK(cudaMalloc(&d->base, image_b));

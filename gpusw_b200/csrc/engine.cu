@@ -1488,24 +1488,49 @@ int gpusw_db_upload(gpusw_ctx* c, const uint8_t* codes, const int32_t* offsets, 
     }
     tr.lap("offsets+pinned");
     char* img = reinterpret_cast<char*>(c->pinned);
-    // offsets are relative to codes[0] in the ABI (like the reference's Encoded)
-    parallel_ranges(n, [&](long long lo, long long hi) { pack_range(codes, offsets, *d, c->pinned, (int)lo, (int)hi); });
-    std::fill(c->pinned + w, c->pinned + nwords, 0u);
-    if (n) {
-      parallel_ranges(n, [&](long long lo, long long hi) {
-        memcpy(img + woff_o + (size_t)lo * 8, d->woff.data() + lo, (size_t)(hi - lo) * 8);
-        memcpy(img + len_o + (size_t)lo * 4, d->len.data() + lo, (size_t)(hi - lo) * 4);
-      });
-    }
-    tr.lap("pack");
     CK(cudaMalloc(&d->base, image_b));
     d->words = reinterpret_cast<uint32_t*>(d->base);
     d->woff_d = reinterpret_cast<long long*>(static_cast<char*>(d->base) + woff_o);
     d->len_d = reinterpret_cast<int*>(static_cast<char*>(d->base) + len_o);
     d->bytes = (int64_t)image_b;
     tr.lap("malloc");
-    CK(cudaMemcpyAsync(d->base, img, image_b, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    try {
+      // Pack in a few chunks of sequences: the staging image is page-locked, so each
+      // chunk's words go to the device (async, in order on the stream) while the pool
+      // packs the next one. A chunk's words are [woff[s0], woff[s1]), contiguous because
+      // word offsets increase with the sequence index.
+      // offsets are relative to codes[0] in the ABI (like the reference's Encoded)
+      const int chunks = n >= (1 << 18) ? 4 : 1;
+      for (int k = 0; k < chunks; ++k) {
+        const int s0 = (int)((long long)n * k / chunks), s1 = (int)((long long)n * (k + 1) / chunks);
+        if (s0 == s1) continue;
+        parallel_ranges(s1 - s0, [&](long long lo, long long hi) {
+          pack_range(codes, offsets, *d, c->pinned, s0 + (int)lo, s0 + (int)hi);
+        });
+        const long long w0 = d->woff[s0], w1 = s1 < n ? d->woff[s1] : w;
+        if (w1 > w0)
+          CK(cudaMemcpyAsync(d->words + w0, c->pinned + w0, (size_t)(w1 - w0) * 4, cudaMemcpyHostToDevice,
+                             c->stream));
+      }
+      std::fill(c->pinned + w, c->pinned + nwords, 0u);
+      if (n) {
+        parallel_ranges(n, [&](long long lo, long long hi) {
+          memcpy(img + woff_o + (size_t)lo * 8, d->woff.data() + lo, (size_t)(hi - lo) * 8);
+          memcpy(img + len_o + (size_t)lo * 4, d->len.data() + lo, (size_t)(hi - lo) * 4);
+        });
+      }
+      tr.lap("pack");
+      // the tail: slack words, then word offsets and lengths
+      const size_t tail_o = (size_t)w * 4;
+      CK(cudaMemcpyAsync(static_cast<char*>(d->base) + tail_o, img + tail_o, image_b - tail_o,
+                         cudaMemcpyHostToDevice, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    } catch (...) {
+      cudaStreamSynchronize(c->stream);
+      cudaFree(d->base);
+      d->base = nullptr;
+      throw;
+    }
     tr.lap("copy");
     c->held += d->bytes;
     const int h = c->next_db++;

@@ -6,7 +6,7 @@ import pytest
 
 import oracle
 from gpusw_b200 import Aligner, Matrix, Scheme, align_pairs, align_score
-from gpusw_b200.encode import funnel
+from gpusw_b200.encode import Encoded, funnel
 from tests._util import golden, rand_seqs, scheme_from_spec
 
 pytestmark = pytest.mark.gpu
@@ -197,4 +197,33 @@ def test_pairs_kernel_paths(scheme, alpha, hi):
     al = Aligner(scheme).index(rs).set_queries(qs)
     got = al.score_pairs(qi, rj)
     want = oracle.score_pairs(funnel(qs, scheme), funnel(rs, scheme), qi, rj, scheme)
+    assert np.array_equal(got.astype(np.int64), want)
+
+
+def _short_set(rng, n, max_len, ncodes, alphabet):
+    lengths = rng.integers(0, max_len + 1, size=n).astype(np.int32)
+    offsets = np.zeros(n + 1, dtype=np.int32)
+    np.cumsum(lengths, out=offsets[1:])
+    codes = rng.integers(0, ncodes, size=int(offsets[-1])).astype(np.uint8)
+    return Encoded(codes=codes, offsets=offsets, ids=[f"s{i}" for i in range(n)],
+                   lengths=lengths, alphabet=alphabet)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scheme,ncodes", [
+    (Scheme(mode="semiglobal", free_end_gaps_query=True, free_end_gaps_ref=True), 4),
+    (Scheme(mode="local", matrix=Matrix.named("BLOSUM62"), gap_open=-11, gap_extend=-1), 24),
+], ids=["dna_2bit", "protein_5bit"])
+def test_many_short_sequences_chunked_upload(scheme, ncodes):
+    """Sets of 300,000 sequences (0-32 residues) are packed and copied to the device in
+    chunks that overlap; every pair must still score as the oracle says."""
+    rng = np.random.default_rng(300_000 + ncodes)
+    n = 300_000
+    qs = _short_set(rng, n, 32, ncodes, scheme.eff_alphabet)
+    rs = _short_set(rng, n, 32, ncodes, scheme.eff_alphabet)
+    qi = rng.permutation(n).astype(np.int32)
+    rj = rng.integers(0, n, size=n).astype(np.int32)
+    al = Aligner(scheme).index(rs).set_queries(qs)
+    got = al.score_pairs(qi, rj)
+    want = oracle.score_pairs(qs, rs, qi, rj, scheme)
     assert np.array_equal(got.astype(np.int64), want)

@@ -1495,6 +1495,18 @@ int gpusw_db_upload(gpusw_ctx* c, const uint8_t* codes, const int32_t* offsets, 
     d->bytes = (int64_t)image_b;
     tr.lap("malloc");
     try {
+      // The tail (slack words, then word offsets and lengths) is ready first: it goes to
+      // the device while the first chunk is packed.
+      std::fill(c->pinned + w, c->pinned + nwords, 0u);
+      if (n) {
+        parallel_ranges(n, [&](long long lo, long long hi) {
+          memcpy(img + woff_o + (size_t)lo * 8, d->woff.data() + lo, (size_t)(hi - lo) * 8);
+          memcpy(img + len_o + (size_t)lo * 4, d->len.data() + lo, (size_t)(hi - lo) * 4);
+        });
+      }
+      const size_t tail_o = (size_t)w * 4;
+      CK(cudaMemcpyAsync(static_cast<char*>(d->base) + tail_o, img + tail_o, image_b - tail_o,
+                         cudaMemcpyHostToDevice, c->stream));
       // Pack in a few chunks of sequences: the staging image is page-locked, so each
       // chunk's words go to the device (async, in order on the stream) while the pool
       // packs the next one. A chunk's words are [woff[s0], woff[s1]), contiguous because
@@ -1512,18 +1524,7 @@ int gpusw_db_upload(gpusw_ctx* c, const uint8_t* codes, const int32_t* offsets, 
           CK(cudaMemcpyAsync(d->words + w0, c->pinned + w0, (size_t)(w1 - w0) * 4, cudaMemcpyHostToDevice,
                              c->stream));
       }
-      std::fill(c->pinned + w, c->pinned + nwords, 0u);
-      if (n) {
-        parallel_ranges(n, [&](long long lo, long long hi) {
-          memcpy(img + woff_o + (size_t)lo * 8, d->woff.data() + lo, (size_t)(hi - lo) * 8);
-          memcpy(img + len_o + (size_t)lo * 4, d->len.data() + lo, (size_t)(hi - lo) * 4);
-        });
-      }
       tr.lap("pack");
-      // the tail: slack words, then word offsets and lengths
-      const size_t tail_o = (size_t)w * 4;
-      CK(cudaMemcpyAsync(static_cast<char*>(d->base) + tail_o, img + tail_o, image_b - tail_o,
-                         cudaMemcpyHostToDevice, c->stream));
       CK(cudaStreamSynchronize(c->stream));
     } catch (...) {
       cudaStreamSynchronize(c->stream);

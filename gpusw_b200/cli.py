@@ -5,10 +5,11 @@
     python -m gpusw_b200 pairs --queries q.fasta --refs r.fasta --scheme dna
     python -m gpusw_b200 info
 
-Same subcommands, options and CSV layouts as the reference package's CLI
-(``src/gpusw/cli.py:28-143``); the top-k subcommand streams one query block at a time to
-the CSV and reports GCUPS on stderr, and with ``--coords`` adds the coordinates of each
-hit's best local alignment (the reference recovers those by re-aligning on the CPU).
+The subcommand names, option names and CSV layouts are those of the reference package's
+CLI (``src/gpusw/cli.py:28-143``), so scripts written for it run unchanged. The top-k
+subcommand streams one query block at a time to the CSV and reports GCUPS on stderr; with
+``--coords`` it adds the coordinates of each hit's best local alignment (the reference
+recovers those by re-aligning on the CPU).
 """
 from __future__ import annotations
 
@@ -30,20 +31,33 @@ from .aligner import Aligner
 from .encode import read_fasta
 
 
-def _scoring_args(p: argparse.ArgumentParser) -> None:
-    p.add_argument("--queries", required=True, help="FASTA file of query sequences")
-    p.add_argument("--refs", required=True, help="FASTA file of reference sequences")
-    p.add_argument("--scheme", default="dna", help="preset name (dna, blosum62, ...)")
-    p.add_argument("--mode", choices=["local", "global", "semiglobal"], default=None)
-    p.add_argument("--matrix", default=None, help="named substitution matrix override")
-    p.add_argument("--match", type=int, default=None)
-    p.add_argument("--mismatch", type=int, default=None)
-    p.add_argument("--gap-open", type=int, default=None, dest="gap_open")
-    p.add_argument("--gap-extend", type=int, default=None, dest="gap_extend")
-    p.add_argument("--dtype", choices=["auto", "int16", "int32"], default=None)
-    p.add_argument("--threads", type=int, default=128)
-    p.add_argument("--backend", choices=["auto", "cuda", "metal"], default="auto")
-    p.add_argument("--out", "-o", default="-", help="output CSV path ('-' = stdout)")
+# Options shared by the scoring subcommands: (flags, argparse keywords). The option names
+# and choices are the reference CLI's interface; everything else here is this package's.
+_SCORING_OPTIONS = (
+    (("--queries",), dict(required=True, metavar="FASTA", help="query records (FASTA, may be gzipped)")),
+    (("--refs",), dict(required=True, metavar="FASTA", help="reference records (FASTA, may be gzipped)")),
+    (("--scheme",), dict(default="dna", help="named scoring preset to start from")),
+    (("--mode",), dict(choices=("local", "global", "semiglobal"), default=None,
+                       help="alignment mode (default: the preset's)")),
+    (("--matrix",), dict(default=None, help="bundled substitution matrix replacing the preset's")),
+    (("--match",), dict(type=int, default=None, help="score of identical residues")),
+    (("--mismatch",), dict(type=int, default=None, help="score of differing residues")),
+    (("--gap-open",), dict(type=int, default=None, dest="gap_open",
+                           help="cost of a gap's first residue (<= 0)")),
+    (("--gap-extend",), dict(type=int, default=None, dest="gap_extend",
+                             help="cost of each further gap residue (<= 0)")),
+    (("--dtype",), dict(choices=("auto", "int16", "int32"), default=None,
+                        help="score width policy (default: the preset's)")),
+    (("--threads",), dict(type=int, default=128, help="accepted for compatibility; unused")),
+    (("--backend",), dict(choices=("auto", "cuda", "metal"), default="auto",
+                          help="accepted for compatibility; only CUDA runs")),
+    (("--out", "-o"), dict(default="-", metavar="CSV", help="where to write the CSV (- for stdout)")),
+)
+
+
+def _add_options(p: argparse.ArgumentParser, options) -> None:
+    for flags, kw in options:
+        p.add_argument(*flags, **kw)
 
 
 def _scheme_kw(args) -> dict:
@@ -126,28 +140,37 @@ def _cmd_info(_args) -> int:
     return 0
 
 
-def main(argv=None) -> int:
+# Subcommands: name -> (one-line summary, handler, options of its own).
+_COMMANDS = {
+    "cross": ("score every query against every reference", _cmd_cross, ()),
+    "topk": ("the k best references of each query, streamed in query blocks", _cmd_topk, (
+        (("-k",), dict(type=int, default=5, help="hits kept per query")),
+        (("--block",), dict(type=int, default=4096, help="queries scored per streamed block")),
+        (("--coords",), dict(action="store_true",
+                             help="append 0-based, end-exclusive start/end coordinates of each "
+                                  "hit's best local alignment (local schemes; -1 for score 0)")),
+    )),
+    "pairs": ("score the i-th query against the i-th reference", _cmd_pairs, ()),
+    "info": ("print the version, the CUDA device status and the bundled matrices", _cmd_info, None),
+}
+
+
+def _parser() -> argparse.ArgumentParser:
     ap = argparse.ArgumentParser(prog="gpusw_b200", description=__doc__,
                                  formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--version", action="version", version=f"gpusw_b200 {__version__}")
-    sub = ap.add_subparsers(dest="cmd", required=True)
-    pc = sub.add_parser("cross", help="all-pairs score matrix")
-    _scoring_args(pc)
-    pc.set_defaults(func=_cmd_cross)
-    pt = sub.add_parser("topk", help="per-query top-k references")
-    _scoring_args(pt)
-    pt.add_argument("-k", type=int, default=5)
-    pt.add_argument("--block", type=int, default=4096, help="queries per streamed block")
-    pt.add_argument("--coords", action="store_true",
-                    help="add 0-based, end-exclusive coordinates of each hit's best local "
-                         "alignment (local schemes; -1 where the score is 0)")
-    pt.set_defaults(func=_cmd_topk)
-    pp = sub.add_parser("pairs", help="score queries vs refs 1:1")
-    _scoring_args(pp)
-    pp.set_defaults(func=_cmd_pairs)
-    pi = sub.add_parser("info", help="environment / GPU info")
-    pi.set_defaults(func=_cmd_info)
-    args = ap.parse_args(argv)
+    cmds = ap.add_subparsers(dest="cmd", required=True, metavar="COMMAND")
+    for name, (summary, handler, extra) in _COMMANDS.items():
+        p = cmds.add_parser(name, help=summary, description=summary)
+        if extra is not None:  # None: a command that scores nothing takes no scoring options
+            _add_options(p, _SCORING_OPTIONS)
+            _add_options(p, extra)
+        p.set_defaults(func=handler)
+    return ap
+
+
+def main(argv=None) -> int:
+    args = _parser().parse_args(argv)
     return args.func(args)
 
 

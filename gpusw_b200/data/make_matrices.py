@@ -3,12 +3,14 @@
 The scores must be identical to the reference's (``src/gpusw/data/matrices/*.txt``,
 public NCBI/Biopython tables), so this script parses each of the reference's files and
 writes the same alphabet and integers back out in NCBI text format with a short header of
-our own. It only runs in a checkout that has the reference next to it:
+our own. It needs a checkout of the reference package, whose matrix directory is given as
+the argument or in the environment variable ``GPUSW_REFERENCE_MATRICES``:
 
-    python gpusw_b200/data/make_matrices.py /root/reference/src/gpusw/data/matrices
+    python gpusw_b200/data/make_matrices.py <reference checkout>/src/gpusw/data/matrices
 """
 from __future__ import annotations
 
+import os
 import pathlib
 import sys
 
@@ -45,4 +47,7 @@ def main(src_dir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/gpusw/data/matrices")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GPUSW_REFERENCE_MATRICES")
+    if not src:
+        raise SystemExit("usage: make_matrices.py <reference checkout>/src/gpusw/data/matrices")
+    main(src)

@@ -1,7 +1,8 @@
 """Generate the golden fixtures of tests/golden/ from the reference package itself.
 
-Runs only where the reference checkout is available (it imports ``gpusw`` from
-``/root/reference/src``, pure NumPy, read-only). The outputs are committed so that the tests
+Runs only where a checkout of the reference package is available: it imports ``gpusw``
+(pure NumPy) from the checkout's ``src`` directory, given as the first argument or in the
+environment variable ``GPUSW_REFERENCE_SRC``, and only reads it. The outputs are committed so that the tests
 -- on machines without the reference -- compare against numbers the reference produced:
 
 * scores.json   : ``cpu_reference_score`` / ``cpu_reference_matrix`` on seeded random sets
@@ -12,17 +13,27 @@ Runs only where the reference checkout is available (it imports ``gpusw`` from
 * encode.json   : ``funnel`` codes/offsets/ids for the accepted input forms;
 * topk.json     : ``AlignResult.top_k`` on score matrices with ties.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <reference checkout>/src
 """
 from __future__ import annotations
 
 import json
+import os
 import pathlib
 import sys
 
 import numpy as np
 
-REF_SRC = "/root/reference/src"
+
+
+def _ref_src() -> str:
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GPUSW_REFERENCE_SRC")
+    if not src:
+        raise SystemExit("usage: make_golden.py <reference checkout>/src "
+                         "(or set GPUSW_REFERENCE_SRC)")
+    return src
+
+
 OUT = pathlib.Path(__file__).resolve().parent
 
 
@@ -40,7 +51,7 @@ def scheme_spec(s):
 
 
 def main() -> None:
-    sys.path.insert(0, REF_SRC)
+    sys.path.insert(0, _ref_src())
     import gpusw
     from gpusw import Matrix, Scheme, schemes
     from gpusw.encode import funnel

@@ -34,10 +34,11 @@ _lib = None
 
 
 def build(force: bool = False) -> str:
-    """Compile ``gotoh_oracle.c`` into ``liboracle.so`` next to it (gcc -O2, pthreads)."""
+    """Compile ``gotoh_oracle.c`` into ``liboracle.so`` next to it (gcc -O3, pthreads; no
+    host-specific instruction set, so the library built here runs on any x86-64 host)."""
     if force or not os.path.exists(LIB_PATH) or (
             os.path.getmtime(LIB_PATH) < os.path.getmtime(SRC_PATH)):
-        subprocess.check_call(["gcc", "-O2", "-shared", "-fPIC", "-o", LIB_PATH, SRC_PATH,
+        subprocess.check_call(["gcc", "-O3", "-shared", "-fPIC", "-o", LIB_PATH, SRC_PATH,
                                "-lpthread"])
     return LIB_PATH
 

@@ -59,7 +59,7 @@ static int64_t score_one(const uint8_t *q, int64_t n, const uint8_t *r, int64_t 
         f[j] = ORACLE_NEG;
     }
     f[0] = ORACLE_NEG;
-    int64_t best = 0, corner = ORACLE_NEG, endcol = ORACLE_NEG, endrow = ORACLE_NEG;
+    int64_t best = 0, endcol = ORACLE_NEG;
     for (int64_t i = 1; i <= m; ++i) {
         const int32_t *subrow = s->sub + (int64_t)r[i - 1] * s->ns;
         int64_t hleft;
@@ -69,30 +69,48 @@ static int64_t score_one(const uint8_t *q, int64_t n, const uint8_t *r, int64_t 
         int64_t diag = hp[0];
         hp[0] = hleft;
         int64_t eleft = ORACLE_NEG;
-        for (int64_t j = 1; j <= n; ++j) {
-            int64_t fj = hp[j] + go, fe = f[j] + ge;
-            if (fe > fj) fj = fe;
-            int64_t ej = hleft + go, ee = eleft + ge;
-            if (ee > ej) ej = ee;
-            int64_t h = diag + (int64_t)subrow[q[j - 1]];
-            if (ej > h) h = ej;
-            if (fj > h) h = fj;
-            if (local && h < 0) h = 0;
-            if (h > best) best = h;
-            if (!local) {
-                if (i == m && j == n) corner = h;
-                if (s->free_q && j == n && h > endcol) endcol = h;
-                if (s->free_r && i == m && h > endrow) endrow = h;
+        /* the same cell update in both branches; local mode clamps at 0 and keeps the
+         * running maximum, the others read their result from the last row and column */
+        if (local) {
+            for (int64_t j = 1; j <= n; ++j) {
+                int64_t fj = hp[j] + go, fe = f[j] + ge;
+                fj = fe > fj ? fe : fj;
+                int64_t ej = hleft + go, ee = eleft + ge;
+                ej = ee > ej ? ee : ej;
+                int64_t h = diag + (int64_t)subrow[q[j - 1]];
+                h = ej > h ? ej : h;
+                h = fj > h ? fj : h;
+                h = h < 0 ? 0 : h;
+                best = h > best ? h : best;
+                diag = hp[j];
+                hp[j] = h;
+                f[j] = fj;
+                hleft = h;
+                eleft = ej;
             }
-            diag = hp[j];
-            hp[j] = h;
-            f[j] = fj;
-            hleft = h;
-            eleft = ej;
+        } else {
+            for (int64_t j = 1; j <= n; ++j) {
+                int64_t fj = hp[j] + go, fe = f[j] + ge;
+                fj = fe > fj ? fe : fj;
+                int64_t ej = hleft + go, ee = eleft + ge;
+                ej = ee > ej ? ee : ej;
+                int64_t h = diag + (int64_t)subrow[q[j - 1]];
+                h = ej > h ? ej : h;
+                h = fj > h ? fj : h;
+                diag = hp[j];
+                hp[j] = h;
+                f[j] = fj;
+                hleft = h;
+                eleft = ej;
+            }
+            if (hp[n] > endcol) endcol = hp[n];           /* H(i, n), last query column */
         }
     }
     if (local) return best;
+    const int64_t corner = hp[n];                          /* H(m, n) */
     if (global) return corner;
+    int64_t endrow = ORACLE_NEG;                           /* max_j H(m, j), last ref row */
+    for (int64_t j = 1; j <= n; ++j) endrow = hp[j] > endrow ? hp[j] : endrow;
     int64_t res = corner;
     if (s->free_q && endcol > res) res = endcol;
     if (s->free_r && endrow > res) res = endrow;

@@ -1,28 +1,43 @@
 #!/usr/bin/env python
 """Benchmark of the Gotoh scoring engine on B200: GCUPS (giga DP-cell updates per second).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload 16s|protein|pairs|small]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload 16s|protein|pairs|small|serving]
                     [--impl ours|reference]
 
-Default workload: the 16S-shaped exhaustive search -- 2,000 queries (250-253 nt) against
-20,000 references (~1,400-1,600 nt) made from 300 mutated ancestors, DNA local
+Default (headline) workload: the 16S-shaped exhaustive search -- 2,000 queries (250-253 nt)
+against 20,000 references (~1,400-1,600 nt) made from 300 mutated ancestors, DNA local
 2/-3/-5/-2, int16 with int32 rescoring, per-query top-5 (synthetic, seeded). One step
 scores the whole cross product (1.5e13 cells) and selects the top-5 of every query.
 
+Keys of the headline line (and of every sub-record):
+
 * ``value``: batched form, inputs resident in HBM, device time of the step from CUDA events
   on the engine's stream, L2 flushed (256 MiB memset) before every timed step; summed over
-  K steps and maxed over ranks.
+  the timed steps and maxed over ranks.
 * ``e2e``: the same step through the C ABI with host buffers: upload of the encoded query
-  and reference sets (host -> device), scoring, top-k, copy of the top-k back; wall time.
+  and reference sets (host -> device), scoring, top-k, copy of the results back; wall time.
 * ``plain``: the same kernels in the one-batch-per-call form (16 queries per call, input
-  order, one kernel shape per call, no length binning), for the batched/plain ratio.
-* ``roofline``: the scoring kernels against the int16x2 instruction roofline -- the DPX
-  add-max rate measured live on this GPU x 2 cells / 5.5 instructions per cell pair.
-* ``cpu_baseline`` / ``--impl reference``: the C restatement of the reference's oracle on
-  all host cores, on a bounded seeded sample of the same workload.
+  order, one kernel shape per call, no length binning, no graph), for batched/plain.
+* ``roofline``: the scoring kernels against the int16x2 instruction roofline. Each register
+  of two cells takes 4.5 DPX instructions on the ALU pipe (F, X, E, H and half a running
+  max) and one ``vadd2`` on the FMA pipe; with the DPX rate measured live on this GPU the
+  ALU pipe binds: peak = rate x 2 cells / 4.5.
+* ``cpu_baseline``: the C restatement of the reference's oracle on all host cores, on a
+  bounded seeded sample of the same workload; ``cpu_baseline_ref``: the reference package's
+  own pure-NumPy ``cpu_reference_score`` (installed under baseline/_ref) in a process pool
+  over all host cores, on a seeded sample of at least 1e8 cells (skipped with a reason when
+  the install is absent). Both samples are also checked against the GPU's scores.
 
-With torchrun and N > 1 every rank runs an independent replica of the workload on its own
-GPU (the scoring path has no exchange step); ``value`` = N x cells / max-over-ranks time.
+At N = 1 the default run adds sub-records for the other configurations, each with its own
+steps, clocks and bit-exact check: ``protein`` (4,096 x 100,000 uneven-length BLOSUM62,
+top-10), ``pairs`` (10^6 read/window pairs, semiglobal), ``small`` (32 x 128 DNA, both
+``dtype="auto"`` and ``"int32"``, every score checked against the reference's own code),
+and ``serving`` (64 Poisson requests per offered load over the resident 16S references, each
+request's top-k checked against the same request scored alone).
+
+With torchrun and N > 1 every rank runs an independent replica of the headline workload on
+its own GPU (the scoring path has no exchange step); ``value`` = N x cells / max-over-ranks
+time; the sub-records are skipped.
 """
 from __future__ import annotations
 
@@ -39,10 +54,15 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+REF_INSTALL = os.path.join(ROOT, "baseline", "_ref")
 
 METRIC = "GCUPS on 1 B200 (bit-exact) batched/served vs plain; p50/p99 request latency"
-OPS_PER_CELL_PAIR = 5.5  # int16x2 instructions per register of two cells (see dp_core.cuh)
+# Per int16x2 register of two cells (dp_core.cuh): F, X, E, HGO add-max and half a 3-input
+# running max issue on the ALU pipe; X + go (vadd2) issues on the FMA pipe.
+ALU_OPS_PER_REG = 4.5
+FMA_OPS_PER_REG = 1.0
 L2_FLUSH_BYTES = 256 << 20
+SERVE_LOADS = "0.5,1,2,4,10,100,2000"
 
 
 def parse():
@@ -55,10 +75,11 @@ def parse():
     ap.add_argument("--serve-slots", type=int, default=2)
     ap.add_argument("--serve-batch-cells", type=float, default=0.0,
                     help="server work per batch in cells (0: the engine default)")
-    ap.add_argument("--serve-loads", default="1,4,16",
+    ap.add_argument("--serve-loads", default=SERVE_LOADS,
                     help="offered loads (requests/s) of the serving sweep")
-    ap.add_argument("--serve-requests", type=int, default=8, help="requests per offered load")
+    ap.add_argument("--serve-requests", type=int, default=64, help="requests per offered load")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-sub", action="store_true", help="headline workload only")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=2)
@@ -113,10 +134,10 @@ def aggregate(group, world: int, cells_per_rank: float, steps: int, step_ms: lis
     return world * cells_per_rank * steps / (max_ms * 1e-3) / 1e9, max_ms
 
 
-def workload(name: str, nq=None, nr=None):
+def workload(name: str, nq=None, nr=None, **extra):
     from gpusw_b200 import workloads
 
-    kw = {}
+    kw = dict(extra)
     if name in ("16s", "protein"):
         if nq:
             kw["n_queries"] = nq
@@ -149,6 +170,7 @@ class ClockSampler:
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+        return self
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -176,50 +198,11 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------ CPU side
-def cpu_sample(wl, seconds: float, rng_seed: int = 99):
-    """A seeded subsample of the workload sized to about `seconds` of oracle time on all
-    host threads; returns (q_enc, r_enc, q_idx, r_idx, cells, gcups, threads)."""
-    import oracle
+def _enc(wl, codes, offs):
     from gpusw_b200.encode import Encoded
 
-    def enc(codes, offs):
-        return Encoded(codes, offs, list(range(offs.shape[0] - 1)), np.diff(offs).astype(np.int32),
-                       wl.scheme.eff_alphabet)
-
-    q = enc(*wl.queries)
-    r = enc(*wl.refs)
-    threads = os.cpu_count() or 1
-    rng = np.random.default_rng(rng_seed)
-    if wl.pairs is not None:
-        def run(n):
-            sel = rng.choice(wl.pairs[0].shape[0], size=n, replace=False).astype(np.int32)
-            qi, rj = wl.pairs[0][sel], wl.pairs[1][sel]
-            t0 = time.perf_counter()
-            oracle.score_pairs(q, r, qi, rj, wl.scheme, threads=threads)
-            dt = time.perf_counter() - t0
-            cells = float((q.lengths[qi].astype(np.float64) * r.lengths[rj]).sum())
-            return (qi, rj), cells, dt
-        sample, cells, dt = run(2000)
-        rate = cells / dt
-        n = int(min(wl.pairs[0].shape[0], max(2000, 2000 * seconds * rate / cells)))
-        sample, cells, dt = run(n)
-    else:
-        def run(nq, nr):
-            qi = np.sort(rng.choice(q.n, size=min(nq, q.n), replace=False)).astype(np.int32)
-            rj = np.sort(rng.choice(r.n, size=min(nr, r.n), replace=False)).astype(np.int32)
-            rsub = enc(*subset(wl.refs, rj))
-            t0 = time.perf_counter()
-            oracle.score_cross(q, rsub, wl.scheme, qlist=qi, threads=threads)
-            dt = time.perf_counter() - t0
-            cells = float(q.lengths[qi].astype(np.float64).sum() * rsub.lengths.astype(np.float64).sum())
-            return (qi, rj), cells, dt
-        nq0 = min(q.n, 16)
-        sample, cells, dt = run(nq0, min(r.n, 64))
-        rate = cells / dt
-        target = seconds * rate
-        nr = int(min(r.n, max(64, target / max(1.0, q.lengths.mean() * nq0 * r.lengths.mean()))))
-        sample, cells, dt = run(nq0, nr)
-    return sample, cells, cells / dt / 1e9, threads, dt
+    return Encoded(codes, offs, list(range(offs.shape[0] - 1)), np.diff(offs).astype(np.int32),
+                   wl.scheme.eff_alphabet)
 
 
 def subset(enc_pair, idx):
@@ -231,18 +214,327 @@ def subset(enc_pair, idx):
     return (np.concatenate(parts) if parts else np.zeros(0, np.uint8), new_offs.astype(np.int32))
 
 
+def sample_pairs(wl, rng, n):
+    """A seeded sample of the workload's (query, reference) pairs: for a pairs workload n
+    of its pairs; for a cross product 16 queries x the first references of a seeded
+    permutation, as many as make about n pairs."""
+    if wl.pairs is not None:
+        sel = np.sort(rng.choice(wl.pairs[0].shape[0], size=min(n, wl.pairs[0].shape[0]),
+                                 replace=False))
+        return wl.pairs[0][sel].astype(np.int32), wl.pairs[1][sel].astype(np.int32), None
+    if n >= wl.nq * wl.nr:  # the whole cross product
+        return (np.arange(wl.nq, dtype=np.int32), np.arange(wl.nr, dtype=np.int32),
+                (wl.nq, wl.nr))
+    nq = min(wl.nq, 16)
+    qi = np.sort(rng.choice(wl.nq, size=nq, replace=False)).astype(np.int32)
+    nr = int(min(wl.nr, max(1, n // nq)))
+    rj = np.sort(rng.choice(wl.nr, size=nr, replace=False)).astype(np.int32)
+    return qi, rj, (nq, nr)
+
+
+def pair_cells(wl, qi, rj, grid) -> float:
+    ql = np.diff(wl.queries[1]).astype(np.float64)
+    rl = np.diff(wl.refs[1]).astype(np.float64)
+    if grid is None:
+        return float((ql[qi] * rl[rj]).sum())
+    return float(ql[qi].sum() * rl[rj].sum())
+
+
+def cpu_port(wl, seconds: float, rng_seed: int = 99):
+    """The C restatement of the reference's oracle on all host threads, on a seeded sample
+    sized to about `seconds`; returns (qi, rj, grid, want, cells, gcups, threads, dt)."""
+    import oracle
+
+    q, r = _enc(wl, *wl.queries), _enc(wl, *wl.refs)
+    threads = os.cpu_count() or 1
+
+    def run(n):
+        rng = np.random.default_rng(rng_seed)
+        qi, rj, grid = sample_pairs(wl, rng, n)
+        t0 = time.perf_counter()
+        if grid is None:
+            want = oracle.score_pairs(q, r, qi, rj, wl.scheme, threads=threads)
+        else:
+            want = oracle.score_cross(q, _enc(wl, *subset(wl.refs, rj)), wl.scheme, qlist=qi,
+                                      threads=threads)
+        return qi, rj, grid, want, pair_cells(wl, qi, rj, grid), time.perf_counter() - t0
+
+    n = 2048
+    qi, rj, grid, want, cells, dt = run(n)
+    if dt < seconds / 4:
+        n = int(n * seconds / max(dt, 1e-3))
+        total = wl.pairs[0].shape[0] if wl.pairs is not None else wl.nq * wl.nr
+        qi, rj, grid, want, cells, dt = run(min(n, total))
+    return qi, rj, grid, want, cells, cells / dt / 1e9, threads, dt
+
+
+def _ref_pool_init(path):
+    sys.path.insert(0, path)
+    import gpusw  # noqa: F401  (imported once per worker, outside the timed map)
+
+
+def _ref_pool_score(task):
+    """Worker: the reference package's own cpu_reference_score over a chunk of pairs."""
+    spec, chunk = task
+    import gpusw
+    from gpusw.reference import cpu_reference_score
+
+    matrix = gpusw.Matrix.named(spec.pop("matrix")) if spec.get("matrix") else None
+    spec.pop("matrix", None)
+    scheme = gpusw.Scheme(matrix=matrix, **spec)
+    return [cpu_reference_score(q, r, scheme) for q, r in chunk]
+
+
+def _ref_spec(scheme) -> dict:
+    return {"mode": scheme.mode, "match": scheme.match, "mismatch": scheme.mismatch,
+            "gap_open": scheme.gap_open, "gap_extend": scheme.gap_extend,
+            "matrix": scheme.matrix.name if scheme.matrix is not None else None,
+            "alphabet": scheme.alphabet, "free_end_gaps_query": scheme.free_end_gaps_query,
+            "free_end_gaps_ref": scheme.free_end_gaps_ref, "unknown": scheme.unknown,
+            "case_insensitive": scheme.case_insensitive}
+
+
+_REF_CACHE: dict = {}
+
+
+def cpu_reference_code(wl, min_cells: float, qi=None, rj=None, grid=None, rng_seed: int = 98):
+    """The reference package's own CPU scorer (gpusw.reference.cpu_reference_score, pure
+    NumPy) over a seeded sample of >= `min_cells` cells (or the given pairs), in a spawn
+    process pool over all host cores. Returns (record, qi, rj, grid, scores) or (record,).
+    The same workload and scores (any dtype policy) are scored once per process."""
+    key = (wl.name, wl.seed, wl.nq, wl.nr, min_cells,
+           tuple(sorted((k, str(v)) for k, v in _ref_spec(wl.scheme).items())))
+    if key in _REF_CACHE:
+        return _REF_CACHE[key]
+    _REF_CACHE[key] = out = _cpu_reference_code(wl, min_cells, qi, rj, grid, rng_seed)
+    return out
+
+
+def _cpu_reference_code(wl, min_cells, qi, rj, grid, rng_seed):
+    if not os.path.isdir(os.path.join(REF_INSTALL, "gpusw")):
+        return ({"value": None, "unavailable": "the reference package is not installed under "
+                                               "baseline/_ref"},)
+    import multiprocessing as mp
+
+    if qi is None:
+        rng = np.random.default_rng(rng_seed)
+        ql = float(np.diff(wl.queries[1]).mean())
+        rl = float(np.diff(wl.refs[1]).mean())
+        qi, rj, grid = sample_pairs(wl, rng, int(min_cells / (ql * rl)) + 1)
+    alpha = np.array(list(wl.scheme.eff_alphabet + "?"))
+    qc, qo = wl.queries
+    rc, ro = wl.refs
+
+    def text(codes, offs, i):
+        return "".join(alpha[np.minimum(codes[offs[i]:offs[i + 1]], len(alpha) - 1)])
+
+    if grid is None:
+        pairs = [(text(qc, qo, a), text(rc, ro, b)) for a, b in zip(qi, rj)]
+    else:
+        qt = [text(qc, qo, a) for a in qi]
+        rt = [text(rc, ro, b) for b in rj]
+        pairs = [(a, b) for a in qt for b in rt]
+    cores = os.cpu_count() or 1
+    spec = _ref_spec(wl.scheme)
+    per = max(1, len(pairs) // (cores * 8))
+    tasks = [(dict(spec), pairs[i:i + per]) for i in range(0, len(pairs), per)]
+    with mp.get_context("spawn").Pool(cores, initializer=_ref_pool_init, initargs=(REF_INSTALL,)) as pool:
+        pool.map(_ref_pool_score, [(dict(spec), pairs[:1])] * cores)  # workers up, not timed
+        t0 = time.perf_counter()
+        parts = pool.map(_ref_pool_score, tasks)
+        dt = time.perf_counter() - t0
+    scores = np.array([s for p in parts for s in p], dtype=np.int64)
+    if grid is not None:
+        scores = scores.reshape(len(qi), len(rj))
+    cells = pair_cells(wl, qi, rj, grid)
+    desc = (f"{len(qi)} pairs" if grid is None else f"{len(qi)} queries x {len(rj)} refs")
+    rec = {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": cores, "kind": "reference",
+           "code": "gpusw.reference.cpu_reference_score (reference package, unmodified)",
+           "sample": f"{desc} of the workload, {cells:.3e} cells, {dt:.1f} s"}
+    return rec, qi, rj, grid, scores
+
+
+def gpu_scores(ctx, wl, qdb, rdb, qi, rj, grid, policy):
+    """The GPU's scores of a sample (pairs, or a query x reference grid)."""
+    if grid is None:
+        return ctx.score_pairs(qdb, rdb, qi, rj, policy).astype(np.int64)
+    rd = ctx.upload(*subset(wl.refs, rj))
+    try:
+        return ctx.score_cross(qdb, rd, qi, len(rj), policy).astype(np.int64)
+    finally:
+        ctx.free(rd)
+
+
+# ----------------------------------------------------------------------------- GPU side
 def config_of(wl) -> dict:
-    cfg = {"workload": {"16s": "16S-shaped exhaustive search, top-5",
-                        "protein": "uneven-length protein batch, top-10",
-                        "pairs": "paired semiglobal read scoring",
-                        "small": "small DNA cross product, int32"}[wl.name],
-           "queries": wl.nq, "refs": wl.nr, "cells": wl.cells(), "k": wl.k or None,
-           "scheme": f"{wl.scheme.mode} {'matrix ' + wl.scheme.matrix.name if wl.scheme.matrix is not None else f'{wl.scheme.match}/{wl.scheme.mismatch}'} "
-                     f"gaps {wl.scheme.gap_open}/{wl.scheme.gap_extend}",
-           "dtype_policy": wl.scheme.dtype, "seed": wl.seed, "synthetic": wl.note,
-           "l2": "flushed (256 MiB memset) before every timed step",
-           "parallelism": "replicas"}
-    return cfg
+    s = wl.scheme
+    table = f"matrix {s.matrix.name}" if s.matrix is not None else f"{s.match}/{s.mismatch}"
+    return {"workload": {"16s": "16S-shaped exhaustive search, top-5",
+                         "protein": "uneven-length protein batch, top-10",
+                         "pairs": "paired semiglobal read scoring",
+                         "small": "small DNA cross product"}[wl.name],
+            "queries": wl.nq, "refs": wl.nr, "cells": wl.cells(), "k": wl.k or None,
+            "scheme": f"{s.mode} {table} gaps {s.gap_open}/{s.gap_extend}",
+            "dtype_policy": s.dtype, "seed": wl.seed, "synthetic": wl.note,
+            "l2": "flushed (256 MiB memset) before every timed step",
+            "parallelism": "replicas"}
+
+
+def packed_bytes(offs: np.ndarray, bits: int) -> int:
+    per = 6 if bits == 5 else 32 // bits
+    lens = np.diff(offs).astype(np.int64)
+    words = ((lens + per - 1) // per + 3) // 4 * 4
+    return int(words.sum() * 4 + 64 * 4 + lens.shape[0] * 20)
+
+
+def roofline(cells, score_ms, dpx, wl=None, bits=None):
+    """Scoring kernels against the per-pipe instruction ceilings (GCUPS)."""
+    alu = dpx * 2.0 / ALU_OPS_PER_REG / 1e9
+    fma = dpx * 2.0 / FMA_OPS_PER_REG / 1e9
+    achieved = cells / (score_ms * 1e-3) / 1e9 if score_ms > 0 else 0.0
+    traffic, src = None, ("not extrapolated: the references (packed words and stream bytes) "
+                          "are L2-resident and reused by every query pair")
+    if wl is not None and wl.pairs is not None and bits is not None:
+        # the pairs kernel reads each pair's packed words once plus 12 B of per-sequence
+        # metadata, 8 B of pair indices and 4 B of output (the ncu capture of 100,000 such
+        # pairs read 14.9 MB, 1.6 x the packed words, from this metadata and 32-byte sectors)
+        n = wl.pairs[0].shape[0]
+        traffic = float(packed_bytes(wl.queries[1], bits) + packed_bytes(wl.refs[1], bits) + 12 * n)
+        src = "algorithmic bytes of the launch (packed words + metadata + indices + output)"
+    return {"bound": "int", "achieved": achieved, "peak": alu, "unit": "GCUPS",
+            "frac": achieved / alu if alu else None, "peak_pipe": "alu",
+            "ceilings_gcups": {"alu": alu, "fma": fma},
+            "peak_source": (f"measured s16x2 DPX rate {dpx / 1e12:.2f} T lane-ops/s (live, this GPU)"
+                            f" x 2 cells / {ALU_OPS_PER_REG} ALU-pipe ops per register"),
+            "traffic": traffic, "traffic_source": src}
+
+
+def measure(ctx, group, world, local, wl, *, steps, warmup, plain_steps, e2e_steps,
+            e2e_warmup=1, cpu_seconds=0.0, ref_cells=0.0, dpx=0.0, plain_warm_queries=None):
+    """One workload: batched (timed), plain, end to end, roofline, CPU baselines and a
+    bit-exact sample. Every rank runs it; the record is rank 0's view."""
+    ctx.set_scheme(wl.scheme)
+    qdb = ctx.upload(*wl.queries)
+    rdb = ctx.upload(*wl.refs)
+    policy = wl.scheme.dtype
+    qlist = np.arange(wl.nq, dtype=np.int32)
+    cells = wl.cells()
+    small = wl.name == "small"
+
+    def step():
+        if wl.pairs is not None:
+            ctx.score_pairs(qdb, rdb, wl.pairs[0], wl.pairs[1], policy)
+        elif small:
+            ctx.score_cross(qdb, rdb, qlist, wl.nr, policy)
+        else:
+            ctx.topk(qdb, rdb, qlist, wl.nr, wl.k, policy)
+        return ctx.stats()
+
+    # the engine records a call's plan as a CUDA graph on the second call with the same key
+    # and replays it from the third: at least two untimed calls precede the timed ones
+    for _ in range(max(warmup, 2)):
+        step()
+    ctx.sync()
+    group.barrier()
+    sampler = ClockSampler(local).start()
+    times, score_ms, topk_ms, launches, ovf = [], [], [], 0, 0
+    for _ in range(steps):
+        ctx.flush_l2(L2_FLUSH_BYTES)
+        st = step()
+        times.append(st.last_kernel_ms)
+        score_ms.append(st.last_score_ms)
+        topk_ms.append(st.last_topk_ms)
+        launches += st.last_launches
+        ovf += st.last_overflow
+    ctx.sync()
+    group.barrier()
+    clocks = sampler.stop()
+    value, total_ms = aggregate(group, world, cells, steps, times)
+
+    plain = None
+    if plain_steps > 0:
+        ctx.set_options(plain=True)
+        if plain_warm_queries:  # a short call builds the plain form's buffers
+            if small or wl.pairs is not None:
+                step()
+            else:
+                ctx.topk(qdb, rdb, qlist[:plain_warm_queries], wl.nr, wl.k, policy)
+        else:
+            step()
+        pt = []
+        for _ in range(plain_steps):
+            ctx.flush_l2(L2_FLUSH_BYTES)
+            pt.append(step().last_kernel_ms)
+        ctx.set_options(plain=False)
+        p_ms = group.max(sum(pt))
+        plain = {"value": world * cells * plain_steps / (p_ms * 1e-3) / 1e9, "unit": "GCUPS",
+                 "steps": plain_steps,
+                 "form": ("16 queries per batch with results copied back per batch"
+                          if wl.pairs is None else "pairs in input order") +
+                         ", one kernel shape per call sized to its longest query, no length"
+                         " binning, no CUDA graph; device time"}
+
+    # end to end through the C ABI with host buffers
+    e2e_t, h2d, d2h = [], 0, 0
+    for it in range(e2e_steps + (e2e_warmup if e2e_steps > 0 else 0)):
+        ctx.sync()
+        t0 = time.perf_counter()
+        q2 = ctx.upload(*wl.queries)
+        r2 = ctx.upload(*wl.refs)
+        if wl.pairs is not None:
+            res = ctx.score_pairs(q2, r2, wl.pairs[0], wl.pairs[1], policy)
+            d2h, h2d_extra = res.nbytes, wl.pairs[0].nbytes * 2
+        elif small:
+            res = ctx.score_cross(q2, r2, qlist, wl.nr, policy)
+            d2h, h2d_extra = res.nbytes, qlist.nbytes
+        else:
+            idx, sc = ctx.topk(q2, r2, qlist, wl.nr, wl.k, policy)
+            d2h, h2d_extra = idx.nbytes + sc.nbytes, qlist.nbytes
+        if it >= e2e_warmup:
+            e2e_t.append(time.perf_counter() - t0)
+        h2d = packed_bytes(wl.queries[1], ctx.bits(q2)) + packed_bytes(wl.refs[1], ctx.bits(r2)) + h2d_extra
+        ctx.free(q2)
+        ctx.free(r2)
+    e2e = None
+    if e2e_t:
+        e_s = group.max(sum(e2e_t))
+        e2e = {"value": world * cells * len(e2e_t) / e_s / 1e9, "unit": "GCUPS",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": [round(t * 1e3, 2) for t in e2e_t], "warmup": e2e_warmup,
+               "timing": "wall clock around upload + score + top-k + copy back"}
+
+    rec = {"value": value, "unit": "GCUPS", "steps": steps, "warmup": max(warmup, 2),
+           "ms_per_step": total_ms / steps, "gpu_launches": launches,
+           "roofline": roofline(cells, sum(score_ms) / steps, dpx, wl, ctx.bits(qdb)),
+           "plain": plain, "batched_over_plain": (value / plain["value"]) if plain else None,
+           "e2e": e2e, "overflow_rescored": ovf, "clocks": clocks,
+           "config": config_of(wl)}
+    rec["roofline"]["kernel_ms_per_step"] = sum(score_ms) / steps
+    rec["roofline"]["topk_ms_per_step"] = sum(topk_ms) / steps
+
+    # CPU baselines and bit-exact checks of their samples (rank 0, N = 1)
+    rank = int(os.environ.get("RANK", 0))
+    if rank == 0 and world == 1 and cpu_seconds > 0:
+        qi, rj, grid, want, c_cells, c_gcups, threads, c_dt = cpu_port(wl, cpu_seconds)
+        got = gpu_scores(ctx, wl, qdb, rdb, qi, rj, grid, policy)
+        desc = (f"{len(qi)} pairs" if grid is None else f"{len(qi)} queries x {len(rj)} refs")
+        rec["cpu_baseline"] = {"value": c_gcups, "unit": "GCUPS", "cores": threads, "kind": "port",
+                               "sample": f"{desc} of the workload, {c_cells:.3e} cells, {c_dt:.1f} s"}
+        rec["bitexact_sample"] = {"pairs_checked": int(np.asarray(want).size),
+                                  "equal": bool(np.array_equal(got, want)),
+                                  "against": "C restatement of the reference oracle"}
+    if rank == 0 and world == 1 and ref_cells > 0:
+        out = cpu_reference_code(wl, ref_cells)
+        rec["cpu_baseline_ref"] = out[0]
+        if len(out) > 1:
+            _, qi, rj, grid, want = out
+            got = gpu_scores(ctx, wl, qdb, rdb, qi, rj, grid, policy)
+            rec["bitexact_ref_sample"] = {"pairs_checked": int(want.size),
+                                          "equal": bool(np.array_equal(got, want)),
+                                          "against": "gpusw.reference.cpu_reference_score"}
+    ctx.free(qdb)
+    ctx.free(rdb)
+    return rec
 
 
 def run_reference(args, rank):
@@ -255,11 +547,12 @@ def run_reference(args, rank):
     threads = os.cpu_count() or 1
     sample_desc = ""
     for s in range(args.warmup + args.steps):
-        sample, cells, gcups, threads, dt = cpu_sample(wl, min(args.cpu_seconds, 10.0), rng_seed=1000 + s)
+        qi, rj, grid, _, cells, gcups, threads, dt = cpu_port(wl, min(args.cpu_seconds, 10.0),
+                                                              rng_seed=1000 + s)
         if s >= args.warmup:
             per_step.append((cells, dt))
-        sample_desc = (f"{len(sample[0])} x {len(sample[1])} seeded subsample per step" if wl.pairs is None
-                       else f"{len(sample[0])} seeded pairs per step")
+        sample_desc = (f"{len(qi)} x {len(rj)} seeded subsample per step" if grid is not None
+                       else f"{len(qi)} seeded pairs per step")
     cells = sum(c for c, _ in per_step)
     secs = sum(t for _, t in per_step)
     v = cells / secs / 1e9
@@ -273,29 +566,25 @@ def run_reference(args, rank):
     print(json.dumps(out), flush=True)
 
 
-def packed_bytes(offs: np.ndarray, bits: int) -> int:
-    per = 6 if bits == 5 else 32 // bits
-    lens = np.diff(offs).astype(np.int64)
-    words = ((lens + per - 1) // per + 3) // 4 * 4
-    return int(words.sum() * 4 + 64 * 4 + lens.shape[0] * 20)
-
-
-def serving_sweep(aligner, loads, n_requests, seed=4, slots=2, k=10, batch_cells=0.0):
+# ------------------------------------------------------------------------------ serving
+def serving_sweep(aligner, loads, reqs, seed=4, slots=2, k=10, batch_cells=0.0, keep=False):
     """Poisson request stream at each offered load against the resident references of
-    `aligner`; latencies (submit -> done) and sustained GCUPS come from the native server."""
+    `aligner`; latencies (submit -> done) and sustained GCUPS come from the native server.
+    With keep=True every load's per-request top-k results are returned as well."""
     import threading
 
-    from gpusw_b200 import workloads
     from gpusw_b200.encode import Encoded
     from gpusw_b200.server import Server
 
-    reqs = workloads.requests(seed=seed, n_requests=n_requests)
     sch = aligner.scheme
     encs = [Encoded(c, o, list(range(o.shape[0] - 1)), np.diff(o).astype(np.int32), sch.eff_alphabet)
             for c, o in reqs]
+    cells_per_req = [float(np.diff(o).sum()) * float(np.diff(aligner._refs.offsets).sum())
+                     for _, o in reqs]
     rng = np.random.default_rng(seed + 1)
-    out = []
+    out, kept = [], []
     for lam in loads:
+        results = {}
         with Server(aligner, k=k, slots=slots, max_batch_queries=1024, batch_cells=batch_cells) as srv:
             gaps = rng.exponential(1.0 / lam, size=len(encs))
             ids, done = [], []
@@ -305,42 +594,44 @@ def serving_sweep(aligner, loads, n_requests, seed=4, slots=2, k=10, batch_cells
                     if not ids:
                         time.sleep(0.001)
                         continue
-                    rid = ids.pop(0)
-                    srv.result(rid, timeout=900)
+                    pos, rid = ids.pop(0)
+                    results[pos] = srv.result(rid, timeout=900)
                     done.append(rid)
 
             t0 = time.perf_counter()
             th = threading.Thread(target=collect)
             th.start()
             t_next = t0
-            for e, g in zip(encs, gaps):
+            for pos, (e, g) in enumerate(zip(encs, gaps)):
                 t_next += g
                 delay = t_next - time.perf_counter()
                 if delay > 0:
                     time.sleep(delay)
-                rid = srv.submit(e)
-                ids.append(rid)
+                ids.append((pos, srv.submit(e)))
             th.join(timeout=1800)
             st = srv.stats()
+        if keep:
+            kept.append(results)
+        offered_cells = lam * statistics.fmean(cells_per_req)
         out.append({"offered_rps": lam, "requests": len(encs), "completed": st["completed"],
+                    "regime": "below saturation" if offered_cells < 4e12 else "queueing (above saturation)",
                     "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
                     "max_ms": st["max_ms"], "gcups": st["gcups"],
+                    "offered_gcups": offered_cells / 1e9,
                     "achieved_rps": st["completed"] / st["wall_s"] if st["wall_s"] else None,
                     "batches": st["batches"], "mean_batch_queries": st["mean_batch_queries"]})
-    return out
+    return out, kept
 
 
-def plain_over_requests(aligner, n_requests, seed=4, k=10):
-    """The plain form over the same request stream as `serving_sweep`: every request's top-k
+def plain_over_requests(aligner, reqs, k=10):
+    """The plain form over the same requests as `serving_sweep`: every request's top-k
     computed by itself, one request after another, with the engine's plain form (16-query
     batches in input order, one kernel shape per batch sized to its longest query, no
-    binning, no graph). Device GCUPS (CUDA events around each call)."""
-    from gpusw_b200 import workloads
-
-    reqs = workloads.requests(seed=seed, n_requests=n_requests)
+    binning, no graph). Returns (device GCUPS, per-request (idx, scores))."""
     ctx = aligner._ctx()
     ref_res = float(np.diff(aligner._refs.offsets).sum())
     cells = ms = 0.0
+    alone = []
     with ctx.lock:
         ctx.set_scheme(aligner.scheme)
         ctx.set_options(plain=True)
@@ -348,214 +639,111 @@ def plain_over_requests(aligner, n_requests, seed=4, k=10):
             for codes, offs in reqs:
                 nq = offs.shape[0] - 1
                 q = ctx.upload(codes, offs)
-                ctx.topk(q, aligner._dref.handle, np.arange(nq, dtype=np.int32), aligner._refs.n, k,
-                         aligner._policy())
+                alone.append(ctx.topk(q, aligner._dref.handle, np.arange(nq, dtype=np.int32),
+                                      aligner._refs.n, k, aligner._policy()))
                 ms += ctx.stats().last_kernel_ms
                 cells += float(np.diff(offs).sum()) * ref_res
                 ctx.free(q)
         finally:
             ctx.set_options(plain=False)
-    return cells / (ms * 1e-3) / 1e9
+    return cells / (ms * 1e-3) / 1e9, alone
+
+
+def serving_record(wl, local, loads, n_requests, slots, batch_cells):
+    from gpusw_b200 import Aligner, workloads
+    from gpusw_b200.encode import Encoded
+
+    refs = Encoded(wl.refs[0], wl.refs[1], list(range(wl.nr)), np.diff(wl.refs[1]).astype(np.int32),
+                   wl.scheme.eff_alphabet)
+    al = Aligner(wl.scheme, device=local).index(refs)
+    reqs = workloads.requests(seed=4, n_requests=n_requests)
+    sampler = ClockSampler(local).start()
+    sweep, served = serving_sweep(al, loads, reqs, slots=slots, batch_cells=batch_cells, keep=True)
+    clocks = sampler.stop()
+    plain, alone = plain_over_requests(al, reqs)
+    for row, res in zip(sweep, served):
+        row["bitexact_requests"] = sum(
+            1 for i, (idx, sc) in enumerate(alone)
+            if i in res and np.array_equal(res[i][0], idx) and np.array_equal(res[i][1], sc))
+    top = max(sweep, key=lambda r: r["gcups"])
+    return {"config": {"workload": "serving over the resident 16S reference set, top-10",
+                       "refs": wl.nr, "requests_per_load": n_requests, "slots": slots,
+                       "batch_cells": batch_cells or "engine default",
+                       "request_queries": "1-512 log-uniform, lengths U[50,2000]"},
+            "sweep": sweep, "best_gcups": top["gcups"],
+            "plain": {"value": plain, "unit": "GCUPS",
+                      "form": "the same requests one at a time, engine plain form (16-query "
+                              "batches, one shape per batch sized to its longest query, no "
+                              "binning, no graph); device time"},
+            "served_over_plain": top["gcups"] / plain if plain > 0 else None,
+            "bitexact_requests": {"checked": len(alone) * len(sweep),
+                                  "equal": sum(r["bitexact_requests"] for r in sweep),
+                                  "against": "each request's top-k scored alone (plain form), "
+                                             "at every offered load"},
+            "clocks": clocks}
 
 
 def run_serving(args, rank, world, local):
     """--workload serving: the serving sweep alone (16S reference set resident)."""
-    from gpusw_b200 import Aligner
-    from gpusw_b200.encode import Encoded
-
     wl = workload("16s", None, args.nr)
-    refs = Encoded(wl.refs[0], wl.refs[1], list(range(wl.nr)), np.diff(wl.refs[1]).astype(np.int32),
-                   wl.scheme.eff_alphabet)
-    al = Aligner(wl.scheme, device=local).index(refs)
     loads = [float(x) for x in args.serve_loads.split(",")]
-    sweep = serving_sweep(al, loads, args.serve_requests, slots=args.serve_slots,
-                          batch_cells=args.serve_batch_cells)
-    plain = plain_over_requests(al, args.serve_requests)
+    rec = serving_record(wl, local, loads, args.serve_requests, args.serve_slots,
+                         args.serve_batch_cells)
     if rank == 0:
-        top = max(sweep, key=lambda r: r["gcups"])
-        print(json.dumps({"metric": METRIC, "value": top["gcups"], "unit": "GCUPS", "n_gpus": world,
-                          "steps": len(sweep), "warmup": 0, "higher_is_better": True,
-                          "scaling": "weak", "vs_baseline": None, "dtype": "int16x2 (int32 rescoring)",
-                          "data": "synthetic",
-                          "config": {"workload": "serving over the resident 16S reference set, top-10",
-                                     "refs": wl.nr, "requests_per_load": args.serve_requests,
-                                     "slots": args.serve_slots,
-                                     "batch_cells": args.serve_batch_cells or "engine default",
-                                     "request_queries": "1-512 log-uniform, lengths U[50,2000]"},
-                          "plain": {"value": plain, "unit": "GCUPS",
-                                    "form": "the same requests one at a time, engine plain form "
-                                            "(16-query batches, one shape per batch sized to its "
-                                            "longest query, no binning, no graph); device time"},
-                          "served_over_plain": top["gcups"] / plain if plain > 0 else None,
-                          "serving": sweep}), flush=True)
+        print(json.dumps({"metric": METRIC, "value": rec["best_gcups"], "unit": "GCUPS",
+                          "n_gpus": world, "steps": len(loads), "warmup": 0,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "int16x2 (int32 rescoring)", "data": "synthetic",
+                          **rec}), flush=True)
 
 
+# --------------------------------------------------------------------------------- main
 def run_ours(args, rank, world, local):
     from gpusw_b200 import _native
 
     group = Group(world)
-    wl = workload(args.workload, args.nq, args.nr)
     ctx = _native.context(local)
-    ctx.set_scheme(wl.scheme)
-    qdb = ctx.upload(*wl.queries)
-    rdb = ctx.upload(*wl.refs)
-    policy = wl.scheme.dtype
-    qlist = np.arange(wl.nq, dtype=np.int32)
-    cells = wl.cells()
-
-    def step():
-        if wl.pairs is not None:
-            ctx.score_pairs(qdb, rdb, wl.pairs[0], wl.pairs[1], policy)
-        else:
-            ctx.topk(qdb, rdb, qlist, wl.nr, wl.k, policy)
-        return ctx.stats()
-
     dpx = ctx.dpx_rate()
-    # the engine records a call's plan as a CUDA graph on the second call with the same key
-    # and replays it from the third: at least two untimed calls precede the timed ones
-    for _ in range(max(args.warmup, 2)):
-        step()
-    sampler = ClockSampler(local)
-    ctx.sync()
-    group.barrier()
-    sampler.start()
-    times, call_ms, score_ms, topk_ms, launches, ovf = [], [], [], [], 0, 0
-    for _ in range(args.steps):
-        ctx.flush_l2(L2_FLUSH_BYTES)
-        st = step()
-        times.append(st.last_kernel_ms)
-        call_ms.append(st.last_total_ms)
-        score_ms.append(st.last_score_ms)
-        topk_ms.append(st.last_topk_ms)
-        launches += st.last_launches
-        ovf += st.last_overflow
-    ctx.sync()
-    group.barrier()
-    clocks = sampler.stop()
-    value, total_ms = aggregate(group, world, cells, args.steps, times)
-    kern_gcups = cells * args.steps / (sum(score_ms) * 1e-3) / 1e9
-    peak_gcups = dpx * 2.0 / OPS_PER_CELL_PAIR / 1e9
-
-    # plain (one batch per call) form of the same kernels, timed the same way
-    plain = None
-    if args.plain_steps > 0:
-        ctx.set_options(plain=True)
-        step()
-        pt = []
-        for _ in range(args.plain_steps):
-            ctx.flush_l2(L2_FLUSH_BYTES)
-            pt.append(step().last_kernel_ms)
-        ctx.set_options(plain=False)
-        p_ms = group.max(sum(pt))
-        plain = {"value": world * cells * args.plain_steps / (p_ms * 1e-3) / 1e9, "unit": "GCUPS",
-                 "form": ("16 queries per batch with results copied back per batch" if wl.pairs is None
-                          else "pairs in input order") +
-                         ", one kernel shape per call sized to its longest query, no length binning,"
-                         " no CUDA graph; device time"}
-
-    # end to end through the C ABI with host buffers
-    e2e_t = []
-    h2d = d2h = 0
-    for it in range(args.e2e_steps + (1 if args.e2e_steps > 0 else 0)):  # one untimed warm-up
-        ctx.sync()
-        t0 = time.perf_counter()
-        q2 = ctx.upload(*wl.queries)
-        r2 = ctx.upload(*wl.refs)
-        if wl.pairs is not None:
-            ctx.score_pairs(q2, r2, wl.pairs[0], wl.pairs[1], policy)
-            d2h = wl.pairs[0].shape[0] * 4
-            h2d_extra = wl.pairs[0].nbytes * 3
-        else:
-            idx, sc = ctx.topk(q2, r2, qlist, wl.nr, wl.k, policy)
-            d2h = idx.nbytes + sc.nbytes
-            h2d_extra = qlist.nbytes
-        if it > 0:
-            e2e_t.append(time.perf_counter() - t0)
-        h2d = packed_bytes(wl.queries[1], ctx.bits(q2)) + packed_bytes(wl.refs[1], ctx.bits(r2)) + h2d_extra
-        ctx.free(q2)
-        ctx.free(r2)
-    e2e = None
-    if e2e_t:
-        e_s = group.max(sum(e2e_t))
-        e2e = {"value": world * cells * len(e2e_t) / e_s / 1e9, "unit": "GCUPS",
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "ms_per_step": [round(t * 1e3, 2) for t in e2e_t], "warmup": 1,
-               "timing": "wall clock around upload + score + top-k + copy back"}
-
-    # a short serving sweep over the same resident references (16S workload only)
-    serving = None
-    if wl.name == "16s" and not args.no_serve and args.serve_requests > 0:
-        from gpusw_b200 import Aligner
-        from gpusw_b200.encode import Encoded
-
-        refs = Encoded(wl.refs[0], wl.refs[1], list(range(wl.nr)),
-                       np.diff(wl.refs[1]).astype(np.int32), wl.scheme.eff_alphabet)
-        al = Aligner(wl.scheme, device=local).index(refs)
-        serving = serving_sweep(al, [float(x) for x in args.serve_loads.split(",")],
-                                args.serve_requests, slots=args.serve_slots,
-                                batch_cells=args.serve_batch_cells)
-        del al
-
-    # CPU oracle baseline and a bit-exact check of the same sample (rank 0, N = 1)
-    cpu = None
-    bitexact = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        import oracle
-        from gpusw_b200.encode import Encoded
-
-        sample, c_cells, c_gcups, threads, c_dt = cpu_sample(wl, args.cpu_seconds)
-        cpu = {"value": c_gcups, "unit": "GCUPS", "cores": threads, "kind": "port",
-               "sample": (f"{len(sample[0])} queries x {len(sample[1])} refs of the workload, "
-                          f"{c_cells:.3e} cells, {c_dt:.1f} s" if wl.pairs is None else
-                          f"{len(sample[0])} pairs of the workload, {c_cells:.3e} cells, {c_dt:.1f} s")}
-        # bit-exactness of the GPU on that sample
-        def as_enc(codes, offs):
-            return Encoded(codes, offs, list(range(offs.shape[0] - 1)),
-                           np.diff(offs).astype(np.int32), wl.scheme.eff_alphabet)
-
-        q = as_enc(*wl.queries)
-        if wl.pairs is None:
-            rsub = subset(wl.refs, sample[1])
-            r = as_enc(*rsub)
-            want = oracle.score_cross(q, r, wl.scheme, qlist=sample[0])
-            rd = ctx.upload(*rsub)
-            got = ctx.score_cross(qdb, rd, sample[0], len(sample[1]), policy)
-            ctx.free(rd)
-        else:
-            r = as_enc(*wl.refs)
-            want = oracle.score_pairs(q, r, sample[0], sample[1], wl.scheme)
-            got = ctx.score_pairs(qdb, rdb, sample[0], sample[1], policy)
-        bitexact = {"pairs_checked": int(np.asarray(want).size),
-                    "equal": bool(np.array_equal(np.asarray(got, dtype=np.int64), want))}
-
-    # DRAM bytes of the dominant kernel's launch, from an ncu capture: the pairs kernel reads
-    # each pair's packed codes once (14.89 MB for 100,000 read/window pairs, nothing written
-    # to DRAM), so it scales with the pairs. The streaming kernel's working set (packed
-    # references, stream bytes) is L2-resident and reused by every query pair, so a small
-    # capture (6.1 MB read for 1.9e11 cells) does not scale and is not extrapolated.
-    traffic, traffic_src = None, "not extrapolated: L2-resident working set (see profiles/)"
-    if wl.pairs is not None:
-        traffic = 14.89e6 / 1e5 * wl.pairs[0].shape[0]
-        traffic_src = "ncu dram__bytes_read+write for 100,000 pairs, scaled by the pairs"
-
+    wl = workload(args.workload, args.nq, args.nr)
+    headline = measure(ctx, group, world, local, wl, steps=args.steps, warmup=args.warmup,
+                       plain_steps=args.plain_steps, e2e_steps=args.e2e_steps,
+                       cpu_seconds=0.0 if args.no_cpu else args.cpu_seconds,
+                       ref_cells=0.0 if args.no_cpu else 1.2e8, dpx=dpx)
+    subs = {}
+    if world == 1 and not args.no_sub and args.workload == "16s" and args.nq is None:
+        cpu = not args.no_cpu
+        # 4,096 x 100,000 proteins: ~14 s per batched step, ~36 s per plain step
+        subs["protein"] = measure(ctx, group, world, local, workload("protein"), steps=2, warmup=3,
+                                  plain_steps=1, e2e_steps=1, e2e_warmup=0,
+                                  cpu_seconds=6.0 if cpu else 0.0, dpx=dpx,
+                                  plain_warm_queries=16)
+        # 10^6 pairs: ~7 ms per step, so enough steps to span several clock samples
+        subs["pairs"] = measure(ctx, group, world, local, workload("pairs"), steps=200, warmup=3,
+                                plain_steps=20, e2e_steps=10, cpu_seconds=5.0 if cpu else 0.0,
+                                dpx=dpx)
+        sm = workload("small")
+        sm_auto = workload("small")
+        sm_auto.scheme = sm.scheme.replace(dtype="auto")
+        subs["small"] = {
+            "int32": measure(ctx, group, world, local, sm, steps=20, warmup=3, plain_steps=5,
+                             e2e_steps=5, dpx=dpx, ref_cells=1e12 if cpu else 0.0),
+            "auto": measure(ctx, group, world, local, sm_auto, steps=20, warmup=3, plain_steps=5,
+                            e2e_steps=5, dpx=dpx, ref_cells=1e12 if cpu else 0.0)}
+        if not args.no_serve and args.serve_requests > 0:
+            loads = [float(x) for x in args.serve_loads.split(",")]
+            subs["serving"] = serving_record(wl, local, loads, args.serve_requests,
+                                             args.serve_slots, args.serve_batch_cells)
     if rank == 0:
-        out = {"metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world,
-               "steps": args.steps, "warmup": args.warmup,
-               "ms_per_step": total_ms / args.steps,
-               "call_ms_per_step": sum(call_ms) / args.steps, "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": None, "dtype": "int16x2 (int32 rescoring)" if policy != "int32" else "int32",
-               "data": "synthetic", "config": config_of(wl), "gpu_launches": launches,
-               "roofline": {"bound": "int", "achieved": kern_gcups, "peak": peak_gcups,
-                            "unit": "GCUPS", "frac": kern_gcups / peak_gcups,
-                            "traffic": traffic,
-                            "traffic_source": traffic_src,
-                            "peak_source": f"measured s16x2 add-max rate {dpx / 1e12:.2f} Tops/s x 2 cells"
-                                           f" / {OPS_PER_CELL_PAIR} ops (live, this GPU)",
-                            "kernel_ms_per_step": sum(score_ms) / args.steps,
-                            "topk_ms_per_step": sum(topk_ms) / args.steps},
-               "plain": plain, "batched_over_plain": (value / plain["value"]) if plain else None,
-               "e2e": e2e, "cpu_baseline": cpu, "bitexact_sample": bitexact,
-               "overflow_rescored": ovf, "serving": serving, "clocks": clocks}
+        out = {"metric": METRIC, "value": headline["value"], "unit": "GCUPS", "n_gpus": world,
+               "steps": args.steps, "warmup": headline["warmup"],
+               "ms_per_step": headline["ms_per_step"], "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None,
+               "dtype": "int16x2 (int32 rescoring)" if wl.scheme.dtype != "int32" else "int32",
+               "data": "synthetic"}
+        out.update({k: v for k, v in headline.items() if k not in out})
+        if "serving" in subs:
+            out["served_over_plain"] = subs["serving"]["served_over_plain"]
+        out.update(subs)
         print(json.dumps(out), flush=True)
     group.close()
 

@@ -26,3 +26,40 @@ def test_reference_arm_json_line():
     assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert "workload" in d["config"]
+
+
+def test_roofline_binds_on_the_alu_pipe():
+    """Each int16x2 register of two cells takes 4.5 DPX ops on the ALU pipe and one vadd2
+    on the FMA pipe, so the ALU ceiling (rate x 2 / 4.5) is the peak the fraction uses."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    rate = 18.48e12
+    r = bench.roofline(cells=8.0e12, score_ms=1000.0, dpx=rate)
+    assert r["peak_pipe"] == "alu" and r["bound"] == "int"
+    assert abs(r["peak"] - rate * 2 / 4.5 / 1e9) < 1e-6
+    assert r["ceilings_gcups"]["fma"] > r["peak"]
+    assert abs(r["frac"] - 8000.0 / r["peak"]) < 1e-12
+    assert r["traffic"] is None  # cross products: L2-resident references, not extrapolated
+
+
+def test_reference_code_baseline_matches_the_oracle():
+    """The reference package's own cpu_reference_score (installed under baseline/_ref), run
+    in a spawn pool, gives the C oracle's scores on a seeded sample of the small workload."""
+    import pytest
+
+    sys.path.insert(0, ROOT)
+    import numpy as np
+
+    import bench
+    import oracle
+
+    if not os.path.isdir(os.path.join(bench.REF_INSTALL, "gpusw")):
+        pytest.skip("reference package not installed under baseline/_ref")
+    wl = bench.workload("small")
+    rec, qi, rj, grid, got = bench.cpu_reference_code(wl, 1.5e6)
+    assert rec["kind"] == "reference" and rec["value"] > 0 and rec["cores"] >= 1
+    assert grid is not None and got.shape == (len(qi), len(rj))
+    q = bench._enc(wl, *wl.queries)
+    want = oracle.score_cross(q, bench._enc(wl, *bench.subset(wl.refs, rj)), wl.scheme, qlist=qi)
+    assert np.array_equal(got, want)

@@ -2101,21 +2101,27 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 std::mutex g_noalloc_mu;
 void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+// The dynamic shared-memory limit is a per-device attribute of each kernel form (local,
+// left-padded semiglobal, general), so it is raised once per (form, device), under the mutex.
+bool g_noalloc_smem_set[3][kNoAllocMaxDevices] = {};
 
 void noalloc_msg(char* buf, int len, const char* msg) {
   if (buf && len > 0) snprintf(buf, (size_t)len, "%s", msg);
 }
 
 template <bool L, bool LP>
-cudaError_t noalloc_launch(const gsw::NoAllocParams& prm, int grid, int teams, size_t smem,
-                           cudaStream_t st) {
+cudaError_t noalloc_launch(const gsw::NoAllocParams& prm, int dev, int grid, int teams,
+                           size_t smem, cudaStream_t st) {
   auto k = gsw::pairs_noalloc_kernel<16, 16, L, LP>;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(kSmemCap));
-    if (e != cudaSuccess) return e;
-    configured = true;
+  {
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    bool& set = g_noalloc_smem_set[L ? 0 : LP ? 1 : 2][dev];
+    if (!set) {
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)(kSmemCap));
+      if (e != cudaSuccess) return e;
+      set = true;
+    }
   }
   k<<<grid, 16 * teams, smem, st>>>(prm);
   return cudaGetLastError();
@@ -2236,9 +2242,9 @@ extern "C" int gpusw_score_pairs_noalloc(const uint8_t* q_codes, const int32_t* 
                         cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) {
     const bool local = mode == gsw::kModeLocal, lp = mode == gsw::kModeSemi && free_q && free_r;
-    e = local ? noalloc_launch<true, false>(prm, (int)grid, teams, smem, st)
-              : lp ? noalloc_launch<false, true>(prm, (int)grid, teams, smem, st)
-                   : noalloc_launch<false, false>(prm, (int)grid, teams, smem, st);
+    e = local ? noalloc_launch<true, false>(prm, dev, (int)grid, teams, smem, st)
+              : lp ? noalloc_launch<false, true>(prm, dev, (int)grid, teams, smem, st)
+                   : noalloc_launch<false, false>(prm, dev, (int)grid, teams, smem, st);
   }
   int herr[2] = {0, 0};
   if (e == cudaSuccess) e = cudaMemcpyAsync(herr, base + 8, sizeof herr, cudaMemcpyDeviceToHost, st);
@@ -2249,8 +2255,11 @@ extern "C" int gpusw_score_pairs_noalloc(const uint8_t* q_codes, const int32_t* 
   }
   if (herr[0] != 0) {
     char msg[128];
-    snprintf(msg, sizeof msg, herr[0] == 1 ? "pair index out of range at position %d"
-                                           : "row longer than max_len at pair %d", herr[1]);
+    snprintf(msg, sizeof msg,
+             herr[0] == 1   ? "pair index out of range at position %d"
+             : herr[0] == 2 ? "row longer than max_len at pair %d"
+                            : "code >= table side or decreasing offsets at pair %d",
+             herr[1]);
     noalloc_msg(errbuf, errlen, msg);
     return GPUSW_ERR_INVALID;
   }

@@ -520,8 +520,9 @@ __global__ void build_stream_kernel(const Packed rows, const int* __restrict__ o
 // reference package's byte codes and int32 offsets are read in place, scoring is int32
 // (one alignment per lane, so no int16 overflow list is needed), and the work counter,
 // the error word and the boundary strips live in a scratch area whose address the host
-// passes in. Indices and lengths are checked here: a bad pair is recorded in the error
-// word and skipped, its output left untouched.
+// passes in. Indices, lengths and codes are checked here, before any code is used as a
+// table row: a bad pair is recorded in the error word and skipped, its output left
+// untouched.
 struct NoAllocParams {
   SchemeDev S;
   const int* sub;              // ns x ns substitution table in the scratch area
@@ -531,11 +532,22 @@ struct NoAllocParams {
   int n;
   int* out;
   unsigned long long* queue;   // scratch: work counter (zeroed by the host per call)
-  int* err;                    // scratch: [0] = 1 bad index, 2 row longer than a strip; [1] = pair
+  int* err;                    // scratch: [0] = 1 bad index, 2 row longer than a strip,
+                               // 3 code >= ns or decreasing offsets; [1] = pair
   uint2* bnd;                  // scratch: boundary strips, one per team
   int bnd_cap;                 // rows per strip (0: single-pass only)
   int max_len;                 // the caller's bound on every sequence length
 };
+
+// True on every lane of the team when some code of sequence s is >= ns.
+template <int G>
+__device__ __forceinline__ bool team_has_bad_code(const ByteSeqs& seqs, int s, int len, int ns,
+                                                  int lane, unsigned wmask) {
+  const uint8_t* c = seqs.codes + seqs.off[s];
+  bool bad = false;
+  for (int i = lane; i < len; i += G) bad |= (int)__ldg(c + i) >= ns;
+  return __any_sync(wmask, bad) != 0;
+}
 
 template <int G, int W, bool LOCAL, bool LEFTPAD>
 __global__ void __launch_bounds__(256) pairs_noalloc_kernel(const NoAllocParams p) {
@@ -563,8 +575,18 @@ __global__ void __launch_bounds__(256) pairs_noalloc_kernel(const NoAllocParams 
       continue;
     }
     const int n0 = p.cols.length(q), m0 = p.rows.length(r);
+    if (n0 < 0 || m0 < 0) {
+      if (lane == 0 && atomicCAS(p.err, 0, 3) == 0) p.err[1] = k;
+      continue;
+    }
     if (n0 > p.max_len || m0 > p.max_len) {
       if (lane == 0 && atomicCAS(p.err, 0, 2) == 0) p.err[1] = k;
+      continue;
+    }
+    // a code >= ns would index past the profile and the table: check both before use
+    if (team_has_bad_code<G>(p.cols, q, n0, ns, lane, wmask) ||
+        team_has_bad_code<G>(p.rows, r, m0, ns, lane, wmask)) {
+      if (lane == 0 && atomicCAS(p.err, 0, 3) == 0) p.err[1] = k;
       continue;
     }
     Acc acc = init_acc<1>(p.S);

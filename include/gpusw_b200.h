@@ -8,7 +8,8 @@
  * thread, or a lock around it). Host buffers passed in or out belong to the caller.
  *
  * Each entry point names the interface of the reference package (freiburgermsu/gpuSW,
- * Python) that it replaces; see INTEGRATION.md for the ctypes binding.
+ * Python) that it replaces. The package's Python side binds these symbols with ctypes
+ * (gpusw_b200/_native.py).
  */
 #ifndef GPUSW_B200_H
 #define GPUSW_B200_H
@@ -206,8 +207,12 @@ int gpusw_flush_l2(gpusw_ctx *ctx, int64_t bytes);
  * the array and resets its counter and error word; calls that overlap on the GPU (on
  * different streams or threads) race on it and must be serialised by the caller. Runs on
  * `stream` (a cudaStream_t, NULL for the legacy default stream) and returns after the
- * stream is idle. Bad indices or lengths above max_len are found on the device, skipped
- * and reported as GPUSW_ERR_INVALID. Messages go to errbuf (errlen bytes, may be NULL). */
+ * stream is idle. Bad indices, lengths above max_len, decreasing offsets and codes >= ns
+ * are found on the device before any code is used, the pair is skipped (its out[] entry
+ * left as it was) and the call returns GPUSW_ERR_INVALID. Offsets must lie inside the
+ * caller's code buffers (their sizes are not passed, so they cannot be checked). The
+ * shared-memory limit of the kernel is raised once per device, so the first call on each
+ * GPU makes that setting too. Messages go to errbuf (errlen bytes, may be NULL). */
 int gpusw_score_pairs_noalloc(const uint8_t *q_codes, const int32_t *q_offsets, int32_t nq,
                               const uint8_t *r_codes, const int32_t *r_offsets, int32_t nr,
                               const int32_t *qi, const int32_t *rj, int32_t n, int mode,

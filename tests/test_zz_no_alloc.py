@@ -5,14 +5,17 @@ a framework's caching allocator, an arena sized at start-up, a plugin host that 
 allocation in its callbacks. Here the device buffers come from torch, never from the
 engine, and two calls in a row (DNA local with multi-pass columns, then protein semiglobal)
 must return exactly what the allocating entry point (Aligner.score_pairs, i.e.
-gpusw_score_pairs) returns: integer scores, so "within tolerance" means bit-exact. This file
-is collected last so that a failure here never hides the other tests.
+gpusw_score_pairs) returns and what the CPU oracle computes: integer scores, so "within
+tolerance" means bit-exact. This file is collected last so that a failure here never hides
+the other tests.
 """
 import ctypes
+import dataclasses
 
 import numpy as np
 import pytest
 
+import oracle
 from gpusw_b200 import Aligner, Scheme, _native, schemes
 from gpusw_b200.encode import funnel
 from tests._util import rand_seqs
@@ -73,6 +76,7 @@ def test_noalloc_equals_allocating_entry_two_calls_in_a_row():
         assert rc == 0, msg
         want = Aligner(sch).index(rs).set_queries(qs).score_pairs(qi, rj)
         assert np.array_equal(got, want)
+        assert np.array_equal(got, oracle.score_pairs(q, r, qi, rj, sch))
 
 
 def test_noalloc_rejects_bad_inputs_without_touching_outputs():
@@ -91,3 +95,43 @@ def test_noalloc_rejects_bad_inputs_without_touching_outputs():
     rc, got, msg = _noalloc(q, r, qi, rj, sch, max_len=100)  # and the next call is fine
     assert rc == 0, msg
     assert np.array_equal(got, Aligner(sch).index(rs).set_queries(qs).score_pairs(qi, rj))
+
+
+def _with(enc, **kw):
+    return dataclasses.replace(enc, **kw)
+
+
+def test_noalloc_rejects_bad_codes_and_offsets_before_using_them():
+    """A code >= ns would index past the profile and the table; decreasing offsets give a
+    negative length. Both are found on the device before use and the pair is skipped."""
+    sch = schemes.DNA
+    qs, rs, qi, rj = _case(14, sch, "ACGT", 24, 5, 80)
+    q, r = funnel(qs, sch), funnel(rs, sch)
+    ns = sch.substitution_table().shape[0]
+    want = oracle.score_pairs(q, r, qi, rj, sch)
+    # a query code past the table (ns + 5) in the query of pair 3
+    qc = q.codes.copy()
+    qc[q.offsets[qi[3]]] = ns + 5
+    rc, got, msg = _noalloc(_with(q, codes=qc), r, qi, rj, sch, max_len=100)
+    assert rc == _native.E_INVALID and "code" in msg
+    hit = qi == qi[3]
+    assert np.all(got[hit] == -12345)
+    assert np.array_equal(got[~hit], want[~hit])
+    # a reference code of 255 in the reference of pair 5
+    rcodes = r.codes.copy()
+    rcodes[r.offsets[rj[5]]] = 255
+    rc, got, msg = _noalloc(q, _with(r, codes=rcodes), qi, rj, sch, max_len=100)
+    assert rc == _native.E_INVALID and "code" in msg
+    assert np.all(got[rj == rj[5]] == -12345)
+    # decreasing offsets: reference k gets length -1 (k - 1 grows by len(k) + 1 residues,
+    # all of them still inside the buffer since k + 1 is not the last reference)
+    ro = r.offsets.copy()
+    k = next(int(x) for x in rj if 1 <= x < r.n - 1)
+    ro[k] = ro[k + 1] + 1
+    rc, got, msg = _noalloc(q, _with(r, offsets=ro), qi, rj, sch, max_len=200)
+    assert rc == _native.E_INVALID and "offsets" in msg
+    assert np.all(got[rj == k] == -12345)
+    # the shared scratch holds no trace of the failures
+    rc, got, msg = _noalloc(q, r, qi, rj, sch, max_len=100)
+    assert rc == 0, msg
+    assert np.array_equal(got, want)

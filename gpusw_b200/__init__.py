@@ -97,18 +97,12 @@ def align_pairs(queries, refs, *, pairs=None, scheme="dna", mode=None, match=Non
     sch = _build_scheme(scheme, mode=mode, match=match, mismatch=mismatch, gap_open=gap_open,
                         gap_extend=gap_extend, matrix=matrix, alphabet=alphabet,
                         unknown=unknown, dtype=dtype)
-    al = Aligner(sch, threads=threads, backend=backend).index(refs).set_queries(queries)
-    nq, nr = al._queries.n, al._refs.n
-    if pairs is None:
-        if nq != nr:
-            raise ValueError(
-                f"pairs=None requires len(queries)==len(refs) for 1:1 scoring (got {nq} vs "
-                f"{nr}); pass pairs=[(qi, rj), ...]")
-        qi = np.arange(nq, dtype=np.int32)
-        rj = np.arange(nr, dtype=np.int32)
-    else:
-        arr = np.asarray(pairs, dtype=np.int64).reshape(-1, 2) if len(pairs) else \
-            np.zeros((0, 2), dtype=np.int64)
-        qi = arr[:, 0].astype(np.int32)
-        rj = arr[:, 1].astype(np.int32)
+    al = Aligner(sch, threads=threads, backend=backend)
+    if pairs is None:  # 1:1 -- one pipelined upload + score call, nothing kept resident
+        return al.score_zipped(queries, refs, return_ids=return_ids)
+    al.index(refs).set_queries(queries)
+    arr = np.asarray(pairs, dtype=np.int64).reshape(-1, 2) if len(pairs) else \
+        np.zeros((0, 2), dtype=np.int64)
+    qi = arr[:, 0].astype(np.int32)
+    rj = arr[:, 1].astype(np.int32)
     return al.score_pairs(qi, rj, return_ids=return_ids)

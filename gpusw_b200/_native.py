@@ -90,6 +90,10 @@ _SIGNATURES = {
     "gpusw_get_tune": ([_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _I32], ctypes.c_int),
     "gpusw_set_tune": ([_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _I32], ctypes.c_int),
     "gpusw_device_name": ([ctypes.c_int, ctypes.c_char_p, _I32], ctypes.c_int),
+    "gpusw_pack_image": ([_VP, _VP, _I32, _VP, _I64, ctypes.POINTER(_I64), ctypes.POINTER(_I32),
+                          ctypes.POINTER(_I64)], ctypes.c_int),
+    "gpusw_db_upload_image": ([_VP, _VP, _I64, _I32, _I32, _I64, ctypes.POINTER(_I32)], ctypes.c_int),
+    "gpusw_score_pairs_zip": ([_VP, _VP, _VP, _VP, _VP, _I64, ctypes.c_int, _VP], ctypes.c_int),
     "gpusw_score_pairs_noalloc": ([_VP, _VP, _I32, _VP, _VP, _I32, _VP, _VP, _I32, ctypes.c_int,
                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_int, _VP, _I32, _VP, _VP, ctypes.c_char_p, _I32],
@@ -174,6 +178,25 @@ def parse_fasta(data: bytes, lut: np.ndarray, sentinel: int, unknown_error: bool
     finally:
         if h.value:
             lib.gpusw_fasta_free(h)
+
+
+def pack_image(codes: np.ndarray, offsets: np.ndarray) -> tuple[np.ndarray, int, int]:
+    """The engine's packed device image of an encoded set (host only, no GPU needed):
+    ``(image uint8, bits per residue, packed words)``."""
+    lib = load()
+    codes = np.ascontiguousarray(codes, dtype=np.uint8)
+    offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+    n = offsets.shape[0] - 1
+    need, bits, nwords = ctypes.c_int64(0), ctypes.c_int32(0), ctypes.c_int64(0)
+    args = (_ptr(codes), _ptr(offsets), n)
+    outs = (ctypes.byref(need), ctypes.byref(bits), ctypes.byref(nwords))
+    rc = lib.gpusw_pack_image(*args, None, 0, *outs)
+    if rc == OK:
+        image = np.empty(need.value, dtype=np.uint8)
+        rc = lib.gpusw_pack_image(*args, _ptr(image), image.size, *outs)
+    if rc != OK:
+        _raise(rc, lib.gpusw_last_error(None).decode())
+    return image, bits.value, nwords.value
 
 
 def gpu_available() -> bool:
@@ -309,6 +332,14 @@ class Context:
                                              ctypes.byref(h)))
         return h.value
 
+    def upload_image(self, image: np.ndarray, n: int, bits: int, nwords: int) -> int:
+        """Upload a packed image made by :func:`pack_image` (it is checked, not re-packed)."""
+        image = np.ascontiguousarray(image, dtype=np.uint8)
+        h = ctypes.c_int32(0)
+        self._check(self.lib.gpusw_db_upload_image(self.handle, _ptr(image), image.size, int(n),
+                                                   int(bits), int(nwords), ctypes.byref(h)))
+        return h.value
+
     def free(self, db: int) -> None:
         if self.handle:
             self.lib.gpusw_db_free(self.handle, int(db))
@@ -342,6 +373,23 @@ class Context:
         out = np.empty(qi.shape[0], dtype=np.int32)
         self._check(self.lib.gpusw_score_pairs(self.handle, qdb, rdb, _ptr(qi), _ptr(rj),
                                                qi.shape[0], DTYPE_CODES[dtype], _ptr(out)))
+        return out
+
+    def score_pairs_zip(self, q_codes: np.ndarray, q_offsets: np.ndarray, r_codes: np.ndarray,
+                        r_offsets: np.ndarray, dtype: str) -> np.ndarray:
+        """Scores of query i vs reference i from host code bytes and offsets, pipelined
+        (nothing stays resident)."""
+        q_codes = np.ascontiguousarray(q_codes, dtype=np.uint8)
+        r_codes = np.ascontiguousarray(r_codes, dtype=np.uint8)
+        q_offsets = np.ascontiguousarray(q_offsets, dtype=np.int32)
+        r_offsets = np.ascontiguousarray(r_offsets, dtype=np.int32)
+        n = q_offsets.shape[0] - 1
+        if r_offsets.shape[0] - 1 != n:
+            raise ValueError("zipped pairs need as many references as queries")
+        out = np.empty(n, dtype=np.int32)
+        self._check(self.lib.gpusw_score_pairs_zip(self.handle, _ptr(q_codes), _ptr(q_offsets),
+                                                   _ptr(r_codes), _ptr(r_offsets), n,
+                                                   DTYPE_CODES[dtype], _ptr(out)))
         return out
 
     def locate_pairs(self, qdb: int, rdb: int, qi: np.ndarray, rj: np.ndarray, anchored: bool):

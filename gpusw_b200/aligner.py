@@ -16,8 +16,9 @@ import os
 import numpy as np
 
 from . import _native
+from .db import PackedSet
 from .encode import Encoded, funnel
-from .errors import GpuSWError, NoGpuError, SchemeError
+from .errors import EncodeError, GpuSWError, NoGpuError, SchemeError
 from .result import AlignResult
 from .scheme import Scheme
 
@@ -68,10 +69,13 @@ def _reversed_prefixes(enc: Encoded, idx: np.ndarray, plen: np.ndarray):
 class _DeviceSet:
     """A sequence set resident on the device; freed with the owning Aligner."""
 
-    def __init__(self, ctx: _native.Context, enc: Encoded):
+    def __init__(self, ctx: _native.Context, enc):
         self.ctx = ctx
         self.enc = enc
-        self.handle = ctx.upload(enc.codes, enc.offsets)
+        if isinstance(enc, PackedSet):  # a stored packed image: uploaded without re-packing
+            self.handle = ctx.upload_image(enc.image, enc.n, enc.bits, enc.nwords)
+        else:
+            self.handle = ctx.upload(enc.codes, enc.offsets)
 
     def __del__(self):  # pragma: no cover - depends on GC timing
         try:
@@ -109,8 +113,16 @@ class Aligner:
 
     # ------------------------------------------------------------------------ inputs
     def index(self, refs) -> Aligner:
-        """Encode and upload the reference set once; returns ``self``."""
+        """Encode and upload the reference set once; returns ``self``. A
+        :class:`~gpusw_b200.db.PackedSet` (``load_db``) is uploaded as stored."""
         ctx = self._ctx()
+        if isinstance(refs, PackedSet):
+            if refs.alphabet != self.scheme.eff_alphabet:
+                raise EncodeError(f"set alphabet {refs.alphabet!r} != scheme alphabet "
+                                  f"{self.scheme.eff_alphabet!r}")
+            self._refs = refs
+            self._dref = _DeviceSet(ctx, refs)
+            return self
         enc = funnel(refs, self.scheme, id_prefix="r")
         self._refs = enc
         self._dref = _DeviceSet(ctx, enc)
@@ -189,6 +201,30 @@ class Aligner:
         if return_ids:
             return AlignResult(host, [self._queries.ids[i] for i in qi],
                                [self._refs.ids[j] for j in rj], self.scheme)
+        return host
+
+    def score_zipped(self, queries, refs, *, return_ids: bool = False):
+        """Scores of query ``i`` against reference ``i`` -- ``align_pairs`` with
+        ``pairs=None`` (``src/gpusw/__init__.py:145-189``). Both sets are encoded, then
+        packed, uploaded and scored in one pipelined engine call (chunks packed on the host
+        while the GPU scores the previous ones); nothing stays resident, and the aligner's
+        own indexed sets are left as they were. ``(n,)`` int32, or an ``AlignResult``."""
+        r = funnel(refs, self.scheme, id_prefix="r")
+        q = funnel(queries, self.scheme, id_prefix="q")
+        if q.n != r.n:
+            raise ValueError(
+                f"pairs=None requires len(queries)==len(refs) for 1:1 scoring (got {q.n} vs "
+                f"{r.n}); pass pairs=[(qi, rj), ...]")
+        if self.scheme.dtype == "int16":
+            self.scheme.resolve_dtype(max(q.max_len, 1), max(r.max_len, 1))  # may raise
+        policy = self.scheme.dtype if self.scheme.dtype in ("int16", "int32") else "auto"
+        ctx = self._ctx()
+        with ctx.lock:
+            ctx.set_scheme(self.scheme)
+            host = ctx.score_pairs_zip(q.codes, q.offsets, r.codes, r.offsets, policy)
+            self._record(ctx, "sw_pairs")
+        if return_ids:
+            return AlignResult(host, list(q.ids), list(r.ids), self.scheme)
         return host
 
     def top_k(self, queries=None, k: int = 5, *, query_batch: int = 512) -> AlignResult:

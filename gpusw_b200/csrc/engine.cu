@@ -2,6 +2,7 @@
 // launch planner, the int16 -> int32 overflow rescoring and the C ABI of
 // include/gpusw_b200.h.
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cstdlib>
@@ -21,6 +22,11 @@
 
 #include "../../include/gpusw_b200.h"
 #include "kernels.cuh"
+
+#if defined(__x86_64__) && !defined(__CUDA_ARCH__)
+#include <immintrin.h>
+#define GSW_X86_PACK 1
+#endif
 
 namespace {
 
@@ -198,10 +204,14 @@ struct Plan {
 
 }  // namespace
 
+constexpr int kAuxStreams = 3;  // extra streams a call's shape launches fan out to
+
 struct gpusw_ctx {
   int device = 0;
   int sms = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t aux[kAuxStreams] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[kAuxStreams] = {};
   std::string err;
   bool has_scheme = false;
   HostScheme sch;
@@ -221,6 +231,20 @@ struct gpusw_ctx {
   std::vector<std::vector<long long>> seen_keys;  // cacheable keys run once, not yet recorded
   unsigned long long use_clock = 0;
   long long scheme_version = 0;
+  // gpusw_score_pairs_zip: three pipeline slots (page-locked staging, device image, buffers,
+  // completion event); slot 0 runs on `stream`, slots 1 and 2 on aux[0] and aux[1]
+  struct ZipSlot {
+    char* pinned = nullptr;
+    size_t pinned_bytes = 0;
+    int32_t* pinned_out = nullptr;
+    size_t pinned_out_n = 0;
+    DevBuf image;
+    Bufs B;
+    cudaEvent_t done = nullptr;
+    cudaEvent_t tev[4] = {};  // GPUSW_TRACE=1: before/after the image copy, after the kernels and the result copy
+  } zip[3];
+  DevBuf zip_iota;  // 0, 1, 2, ... (the pair index arrays of a chunk)
+  long long zip_iota_n = 0;
   int graphs = 1;              // replay cached plans as CUDA graphs
   int autotune = 1;            // tune stream shapes on first use
   std::vector<std::pair<std::pair<int, int>, std::vector<double>>> tune;  // (ns, P) -> us/row-pass
@@ -320,10 +344,14 @@ class HostPool {
       job_ = &job;
       active_ = nt - 1;
       pending_ = nt - 1;
+      pending_atomic_.store(pending_, std::memory_order_release);
       ++gen_;
     }
+    gen_seen_.store(gen_, std::memory_order_release);
     cv_.notify_all();
     job(0);
+    // the workers finish within microseconds of each other: spin briefly before sleeping
+    for (int spin = 0; spin < kSpin && pending_atomic_.load(std::memory_order_acquire) != 0; ++spin) cpu_relax();
     std::unique_lock<std::mutex> g(mu_);
     done_.wait(g, [&] { return pending_ == 0; });
     job_ = nullptr;
@@ -331,9 +359,19 @@ class HostPool {
   }
 
  private:
+  // Spin iterations (a pause each, ~100 microseconds in all) before a worker or the caller
+  // sleeps on its condition variable: a pipelined call runs several short parallel passes in
+  // a row, and a futex wake-up of every worker costs as much as a pass.
+  static constexpr int kSpin = 20000;
+  static void cpu_relax() {
+#if defined(__x86_64__) && !defined(__CUDA_ARCH__)
+    _mm_pause();
+#endif
+  }
   void loop(int id) {
     unsigned long long seen = 0;
     for (;;) {
+      for (int spin = 0; spin < kSpin && gen_seen_.load(std::memory_order_acquire) == seen; ++spin) cpu_relax();
       const std::function<void(int)>* job;
       {
         std::unique_lock<std::mutex> g(mu_);
@@ -344,7 +382,8 @@ class HostPool {
       }
       (*job)(id + 1);
       std::lock_guard<std::mutex> g(mu_);
-      if (--pending_ == 0) done_.notify_all();
+      pending_atomic_.store(--pending_, std::memory_order_release);
+      if (pending_ == 0) done_.notify_all();
     }
   }
   std::mutex run_mu_, mu_;
@@ -353,6 +392,8 @@ class HostPool {
   const std::function<void(int)>* job_ = nullptr;
   int active_ = 0, pending_ = 0;
   unsigned long long gen_ = 0;
+  std::atomic<unsigned long long> gen_seen_{0};  // gen_, readable without the mutex
+  std::atomic<int> pending_atomic_{0};            // pending_, readable without the mutex
 };
 
 // Run f(begin, end) over [0, n) split into contiguous ranges on the host's cores (one range
@@ -390,40 +431,134 @@ inline uint32_t fold4(uint64_t x) {
   return (uint32_t)(x | (x >> 16));
 }
 
+#if GSW_X86_PACK
+// SSSE3 packing of sequences [s0, s1) at 2 or 4 bits (the same words as the scalar fold2 /
+// fold4 path, checked bit-exact): 16 code bytes become one word at 2 bits (b0 + 4 b1 per byte
+// pair by a multiply-add, 16 x that per pair of pairs by a second one, then the low byte of
+// each 32-bit lane) or two words at 4 bits (b0 + 16 b1 per byte pair, narrowed to bytes). A
+// sequence's last partial block is read by one 16-byte load ending at its last code and moved
+// down by a byte shuffle (shorter sequences copy it to a zeroed buffer), so no load leaves the
+// sequence. The OR of every code byte goes to *or_out.
+__attribute__((target("ssse3"))) inline void fold16_ssse3(__m128i v, int bits, uint32_t* dst) {
+  if (bits == 2) {
+    const __m128i t = _mm_madd_epi16(_mm_maddubs_epi16(v, _mm_set1_epi16(0x0401)), _mm_set1_epi32(0x00100001));
+    const __m128i lanes = _mm_setr_epi8(0, 4, 8, 12, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1);
+    dst[0] = (uint32_t)_mm_cvtsi128_si32(_mm_shuffle_epi8(t, lanes));
+  } else {
+    const __m128i t = _mm_maddubs_epi16(v, _mm_set1_epi16(0x1001));
+    const uint64_t x = (uint64_t)_mm_cvtsi128_si64(_mm_packus_epi16(t, t));
+    memcpy(dst, &x, 8);
+  }
+}
+
+__attribute__((target("ssse3"))) void pack_range_ssse3(const uint8_t* codes, const int32_t* offs,
+                                                       const int* len_of, const long long* woff,
+                                                       int bits, uint32_t* words, int s0, int s1,
+                                                       uint8_t* or_out) {
+  const int per = 32 / bits;
+  const __m128i iota = _mm_setr_epi8(0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15);
+  __m128i acc = _mm_setzero_si128();
+  const int wpb = 16 / per;  // words per 16-code block: 1 at 2 bits, 2 at 4 bits
+  for (int s = s0; s < s1; ++s) {
+    const uint8_t* src = codes + offs[s];
+    const int len = len_of[s];
+    uint32_t* dst = words + woff[s];
+    const long long nw = (((long long)len + per - 1) / per + 3) & ~3ll;
+    const int full = len / 16, tail = len % 16;
+    for (int b = 0; b < full; ++b) {
+      const __m128i v = _mm_loadu_si128(reinterpret_cast<const __m128i*>(src + 16 * b));
+      acc = _mm_or_si128(acc, v);
+      fold16_ssse3(v, bits, dst + (long long)b * wpb);
+    }
+    long long w = (long long)full * wpb;
+    if (tail) {
+      __m128i v;
+      if (len >= 16) {  // bytes [len - 16, len): shift down by 16 - tail, zero the top
+        const __m128i x = _mm_loadu_si128(reinterpret_cast<const __m128i*>(src + len - 16));
+        const __m128i idx = _mm_add_epi8(iota, _mm_set1_epi8((char)(16 - tail)));
+        const __m128i keep = _mm_cmplt_epi8(iota, _mm_set1_epi8((char)tail));
+        v = _mm_and_si128(_mm_shuffle_epi8(x, idx), keep);
+      } else {
+        alignas(16) uint8_t t[16] = {};
+        memcpy(t, src, (size_t)tail);
+        v = _mm_load_si128(reinterpret_cast<const __m128i*>(t));
+      }
+      acc = _mm_or_si128(acc, v);
+      fold16_ssse3(v, bits, dst + w);
+      w += wpb;
+    }
+    for (; w < nw; ++w) dst[w] = 0u;
+  }
+  alignas(16) uint8_t b[16];
+  _mm_store_si128(reinterpret_cast<__m128i*>(b), acc);
+  uint8_t o = 0;
+  for (int i = 0; i < 16; ++i) o |= b[i];
+  *or_out = o;
+}
+
+bool host_has_ssse3() {
+  static const bool v = __builtin_cpu_supports("ssse3");
+  return v;
+}
+#endif
+
 // Pack sequences [s0, s1) into words (each sequence's words including its alignment
-// padding, so the destination needs no prior zeroing).
-void pack_range(const uint8_t* codes, const int32_t* offs, const Db& d, uint32_t* words, int s0, int s1) {
+// padding, so the destination needs no prior zeroing). With or_out, the OR of every code
+// byte packed is stored there: it has a bit at or above `bits` exactly when some code does
+// not fit the width (the words are then wrong and the caller packs again, wider).
+void pack_range(const uint8_t* codes, const int32_t* offs, const Db& d, uint32_t* words, int s0, int s1,
+                uint8_t* or_out = nullptr) {
+  uint8_t orv = 0;
+#if GSW_X86_PACK
+  if ((d.bits == 2 || d.bits == 4) && host_has_ssse3()) {
+    pack_range_ssse3(codes, offs, d.len.data(), d.woff.data(), d.bits, words, s0, s1, &orv);
+    if (or_out) *or_out = orv;
+    return;
+  }
+#endif
   for (int s = s0; s < s1; ++s) {
     const uint8_t* src = codes + offs[s];
     const int len = d.len[s];
     uint32_t* dst = words + d.woff[s];
-    const long long nw = (s + 1 < d.n ? d.woff[s + 1] : d.woff[s] + (((len + d.per - 1) / d.per + 3) & ~3ll)) - d.woff[s];
+    // every sequence holds exactly this many words (data + 16-byte alignment), so a range
+    // never reads the word offset of a sequence outside it (another thread may be writing it)
+    const long long nw = (((long long)len + d.per - 1) / d.per + 3) & ~3ll;
     long long w = 0;
     int c = 0;
     // Whole words of 2-, 4- and 8-bit codes: gather 8 code bytes per 64-bit load and fold
     // neighbouring fields together (codes are below 2^bits, so no masking of the input).
     if (d.bits == 2) {
+      uint64_t o = 0;
       for (; c + 16 <= len; c += 16, ++w) {
         uint64_t a, b;
         memcpy(&a, src + c, 8);
         memcpy(&b, src + c + 8, 8);
+        o |= a | b;
         dst[w] = fold2(a) | (fold2(b) << 16);
       }
+      for (int i = 0; i < 8; ++i) orv |= (uint8_t)(o >> (8 * i));
     } else if (d.bits == 4) {
+      uint64_t o = 0;
       for (; c + 8 <= len; c += 8, ++w) {
         uint64_t a;
         memcpy(&a, src + c, 8);
+        o |= a;
         dst[w] = fold4(a);
       }
+      for (int i = 0; i < 8; ++i) orv |= (uint8_t)(o >> (8 * i));
     } else if (d.bits == 8) {
       for (; c + 4 <= len; c += 4, ++w) memcpy(dst + w, src + c, 4);
     }
     for (; w < nw; ++w) {
       uint32_t v = 0;
-      for (int e = 0; e < d.per && c < len; ++e, ++c) v |= (uint32_t)src[c] << (e * d.bits);
+      for (int e = 0; e < d.per && c < len; ++e, ++c) {
+        orv |= src[c];
+        v |= (uint32_t)src[c] << (e * d.bits);
+      }
       dst[w] = v;
     }
   }
+  if (or_out) *or_out = orv;
 }
 
 Db& get_db(gpusw_ctx* c, int32_t h) {
@@ -439,6 +574,14 @@ void require_scheme(gpusw_ctx* c, const Db& a, const Db& b) {
 }
 
 // -------------------------------------------------------------------------- launches
+// Where one launch goes. Launches of a call that may run concurrently (run_group) get a
+// stream each and disjoint boundary strips, sized by a first pass that launches nothing.
+struct LaunchCfg {
+  cudaStream_t st = nullptr;  // nullptr: the context stream
+  long long bnd_off = -1;     // >= 0: boundary strips at B.bnd + bnd_off (sized beforehand)
+  size_t* need = nullptr;     // sizing pass: store the strip entries needed, launch nothing
+};
+
 // Teams per CTA of the pairs kernel: each team holds its own profile.
 int pair_teams(const Shape& s, int ns) {
   const int t = (int)std::min<size_t>(256 / s.G, kSmemCap / profile_bytes(s, ns));
@@ -446,7 +589,8 @@ int pair_teams(const Shape& s, int ns) {
 }
 
 template <int G, int W, int P, bool L, bool LP, bool LOC = false, bool P8 = false>
-void launch_pairs_t(gpusw_ctx* c, Bufs& B, gsw::PairsParams prm, int /*teams_hint*/, long long max_rows, bool multipass) {
+void launch_pairs_t(gpusw_ctx* c, Bufs& B, gsw::PairsParams prm, int /*teams_hint*/, long long max_rows,
+                    bool multipass, const LaunchCfg& lc = LaunchCfg()) {
   auto k = gsw::pairs_kernel<G, W, P, L, LP, LOC, P8>;
   const Shape s{G, W};
   const size_t sub_bytes = (size_t)(gsw::pairs_sub_uint4(prm.S.ns) + (P8 ? gsw::pairs_ext_uint4(prm.S.ns) : 0)) * 16;
@@ -486,36 +630,41 @@ void launch_pairs_t(gpusw_ctx* c, Bufs& B, gsw::PairsParams prm, int /*teams_hin
   long long grid = (long long)c->sms * std::max(1, bps_best);
   const long long team_items = prm.item_mode == 1 ? kOvfCap : prm.n_items;
   grid = std::max(1ll, std::min(grid, (team_items + teams - 1) / teams));
+  const size_t need = multipass ? (size_t)grid * teams * (size_t)std::max(1ll, max_rows) : 0;
+  if (lc.need) {
+    *lc.need = need;
+    return;
+  }
   if (multipass) {
-    const size_t need = (size_t)grid * teams * (size_t)std::max(1ll, max_rows) * sizeof(uint2);
-    prm.bnd = B.bnd.as<uint2>(need / sizeof(uint2));
+    prm.bnd = lc.bnd_off >= 0 ? static_cast<uint2*>(B.bnd.p) + lc.bnd_off : B.bnd.as<uint2>(need);
     prm.bnd_cap = (int)std::max(1ll, max_rows);
   } else {
     prm.bnd = nullptr;
     prm.bnd_cap = 0;
   }
-  k<<<(int)grid, G * teams, smem, c->stream>>>(prm);
+  k<<<(int)grid, G * teams, smem, lc.st ? lc.st : c->stream>>>(prm);
   CK(cudaGetLastError());
   c->st.last_launches++;
 }
 
 template <int P, bool L, bool LP, bool P8 = false>
-void launch_pairs_shape(gpusw_ctx* c, Bufs& B, int shape, const gsw::PairsParams& prm, int teams, long long max_rows, bool mp) {
+void launch_pairs_shape(gpusw_ctx* c, Bufs& B, int shape, const gsw::PairsParams& prm, int teams, long long max_rows, bool mp,
+                        const LaunchCfg& lc) {
   switch (shape) {
-    case 0: launch_pairs_t<8, 8, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
-    case 1: launch_pairs_t<8, 12, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
-    case 2: launch_pairs_t<8, 16, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
-    case 3: launch_pairs_t<8, 20, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
-    case 4: launch_pairs_t<8, 24, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
-    case 5: launch_pairs_t<16, 16, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
-    case 6: launch_pairs_t<16, 24, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
-    case 7: launch_pairs_t<32, 16, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp); break;
+    case 0: launch_pairs_t<8, 8, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp, lc); break;
+    case 1: launch_pairs_t<8, 12, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp, lc); break;
+    case 2: launch_pairs_t<8, 16, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp, lc); break;
+    case 3: launch_pairs_t<8, 20, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp, lc); break;
+    case 4: launch_pairs_t<8, 24, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp, lc); break;
+    case 5: launch_pairs_t<16, 16, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp, lc); break;
+    case 6: launch_pairs_t<16, 24, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp, lc); break;
+    case 7: launch_pairs_t<32, 16, P, L, LP, false, P8>(c, B, prm, teams, max_rows, mp, lc); break;
     default: fail(GPUSW_ERR_INVALID, "bad pairs kernel shape");
   }
 }
 
 void launch_pairs(gpusw_ctx* c, Bufs& B, int shape, int P, bool local, const gsw::PairsParams& prm,
-                  long long max_rows, bool multipass) {
+                  long long max_rows, bool multipass, const LaunchCfg& lc = LaunchCfg()) {
   const int teams = pair_teams(kPairShapes[shape], prm.S.ns);
   const bool lp = prm.S.mode == gsw::kModeSemi && prm.S.free_q && prm.S.free_r;
   if (P == 2) {
@@ -526,18 +675,18 @@ void launch_pairs(gpusw_ctx* c, Bufs& B, int shape, int P, bool local, const gsw
     const bool p8 = prm.S.s_pad - prm.S.go >= -128 && max_sub - prm.S.go <= 127 &&
                     (local || lp || !(prm.S.mode == gsw::kModeSemi && prm.S.free_q));
     if (p8) {
-      if (local) launch_pairs_shape<2, true, false, true>(c, B, shape, prm, teams, max_rows, multipass);
-      else if (lp) launch_pairs_shape<2, false, true, true>(c, B, shape, prm, teams, max_rows, multipass);
-      else launch_pairs_shape<2, false, false, true>(c, B, shape, prm, teams, max_rows, multipass);
+      if (local) launch_pairs_shape<2, true, false, true>(c, B, shape, prm, teams, max_rows, multipass, lc);
+      else if (lp) launch_pairs_shape<2, false, true, true>(c, B, shape, prm, teams, max_rows, multipass, lc);
+      else launch_pairs_shape<2, false, false, true>(c, B, shape, prm, teams, max_rows, multipass, lc);
       return;
     }
-    if (local) launch_pairs_shape<2, true, false>(c, B, shape, prm, teams, max_rows, multipass);
-    else if (lp) launch_pairs_shape<2, false, true>(c, B, shape, prm, teams, max_rows, multipass);
-    else launch_pairs_shape<2, false, false>(c, B, shape, prm, teams, max_rows, multipass);
+    if (local) launch_pairs_shape<2, true, false>(c, B, shape, prm, teams, max_rows, multipass, lc);
+    else if (lp) launch_pairs_shape<2, false, true>(c, B, shape, prm, teams, max_rows, multipass, lc);
+    else launch_pairs_shape<2, false, false>(c, B, shape, prm, teams, max_rows, multipass, lc);
   } else {
-    if (local) launch_pairs_shape<1, true, false>(c, B, shape, prm, teams, max_rows, multipass);
-    else if (lp) launch_pairs_shape<1, false, true>(c, B, shape, prm, teams, max_rows, multipass);
-    else launch_pairs_shape<1, false, false>(c, B, shape, prm, teams, max_rows, multipass);
+    if (local) launch_pairs_shape<1, true, false>(c, B, shape, prm, teams, max_rows, multipass, lc);
+    else if (lp) launch_pairs_shape<1, false, true>(c, B, shape, prm, teams, max_rows, multipass, lc);
+    else launch_pairs_shape<1, false, false>(c, B, shape, prm, teams, max_rows, multipass, lc);
   }
 }
 
@@ -589,9 +738,51 @@ struct Staging {
   }
 };
 
+// Runs the n shape launches of one call, launch(i, cfg) issuing (or, with cfg.need set,
+// sizing) launch i. A first pass sizes the multi-pass boundary strips of every launch and
+// places them side by side in one allocation; then the launches go out round-robin on the
+// context stream and its auxiliary streams, forked from the context stream's prior work and
+// joined back into it. Launches of different shapes therefore overlap: a small call's
+// few-item launches run side by side instead of one after another, and a large call's
+// launches overlap their last waves. Recorded into a CUDA graph the fork and join become
+// graph edges. The plain form keeps one stream.
+template <class F>
+void run_group(gpusw_ctx* c, Bufs& B, int n, F&& launch) {
+  std::vector<long long> off((size_t)std::max(n, 0), -1);
+  size_t total = 0;
+  for (int i = 0; i < n; ++i) {
+    size_t need = 0;
+    LaunchCfg sz;
+    sz.need = &need;
+    launch(i, sz);
+    if (need) {
+      off[i] = (long long)total;
+      total += need;
+    }
+  }
+  if (total) B.bnd.as<uint2>(total);
+  const int ns = c->plain ? 1 : std::min(n, 1 + kAuxStreams);
+  if (ns > 1) {
+    CK(cudaEventRecord(c->fork_ev, c->stream));
+    for (int a = 0; a + 1 < ns; ++a) CK(cudaStreamWaitEvent(c->aux[a], c->fork_ev, 0));
+  }
+  for (int i = 0; i < n; ++i) {
+    LaunchCfg lc;
+    lc.st = (i % ns == 0) ? c->stream : c->aux[i % ns - 1];
+    lc.bnd_off = off[i];
+    launch(i, lc);
+  }
+  if (ns > 1) {
+    for (int a = 0; a + 1 < ns; ++a) {
+      CK(cudaEventRecord(c->join_ev[a], c->aux[a]));
+      CK(cudaStreamWaitEvent(c->stream, c->join_ev[a], 0));
+    }
+  }
+}
+
 // Overflow rescoring of the int16 cells flagged by the previous launches (int32, any length).
 void launch_overflow_rescore(gpusw_ctx* c, Bufs& B, const Db& q, const Db& r, int* out,
-                             unsigned long long* queue_slot) {
+                             unsigned long long* queue_slot, const LaunchCfg& lc = LaunchCfg()) {
   gsw::PairsParams pp{};
   pp.S = make_scheme(c->sch, 1);
   pp.sub = c->sub_d;
@@ -606,7 +797,7 @@ void launch_overflow_rescore(gpusw_ctx* c, Bufs& B, const Db& q, const Db& r, in
   pp.out = out;
   pp.n_items = kOvfCap;
   const int shape = pick_pair_shape(1 << 30, c->sch.ns);
-  launch_pairs(c, B, shape, 1, c->sch.mode == gsw::kModeLocal, pp, std::max(q.max_len, r.max_len), true);
+  launch_pairs(c, B, shape, 1, c->sch.mode == gsw::kModeLocal, pp, std::max(q.max_len, r.max_len), true, lc);
 }
 
 void run_cross(gpusw_ctx* c, Bufs& B, const Db& q, const Db& r, const int32_t* qlist, int nq, int P,
@@ -694,7 +885,8 @@ const Db::Stream& get_stream(gpusw_ctx* c, Db& r, bool plain) {
 }
 
 template <int G, int W, int P>
-void launch_stream_t(gpusw_ctx* c, Bufs& B, gsw::StreamParams prm, int n_streams_max_total, bool multipass) {
+void launch_stream_t(gpusw_ctx* c, Bufs& B, gsw::StreamParams prm, int n_streams_max_total, bool multipass,
+                     const LaunchCfg& lc) {
   auto k = gsw::cross_stream_kernel<G, W, P>;
   const size_t smem = profile_bytes(Shape{G, W}, prm.S.ns);
   static int configured_dev = -1;
@@ -709,39 +901,46 @@ void launch_stream_t(gpusw_ctx* c, Bufs& B, gsw::StreamParams prm, int n_streams
   long long grid = (long long)c->sms * std::max(1, bps);
   grid = std::max(1ll, std::min<long long>(grid, prm.n_items));
   const int nteams = 256 / G;
+  const long long strip = n_streams_max_total + 2 * gsw::kStreamPadLen;
+  const size_t need = multipass ? (size_t)grid * nteams * strip : 0;
+  if (lc.need) {
+    *lc.need = need;
+    return;
+  }
   if (multipass) {
-    prm.bnd_strip = n_streams_max_total + 2 * gsw::kStreamPadLen;
-    prm.bnd = B.bnd.as<uint2>((size_t)grid * nteams * prm.bnd_strip);
+    prm.bnd_strip = strip;
+    prm.bnd = lc.bnd_off >= 0 ? static_cast<uint2*>(B.bnd.p) + lc.bnd_off : B.bnd.as<uint2>(need);
   } else {
     prm.bnd = nullptr;
     prm.bnd_strip = 0;
   }
-  k<<<(int)grid, 256, smem, c->stream>>>(prm);
+  k<<<(int)grid, 256, smem, lc.st ? lc.st : c->stream>>>(prm);
   CK(cudaGetLastError());
   c->st.last_launches++;
 }
 
 template <int P>
-void launch_stream_shape(gpusw_ctx* c, Bufs& B, int shape, const gsw::StreamParams& prm, int mt, bool mp) {
+void launch_stream_shape(gpusw_ctx* c, Bufs& B, int shape, const gsw::StreamParams& prm, int mt, bool mp,
+                         const LaunchCfg& lc = LaunchCfg()) {
   switch (shape) {
-    case 0: launch_stream_t<8, 4, P>(c, B, prm, mt, mp); break;
-    case 1: launch_stream_t<8, 8, P>(c, B, prm, mt, mp); break;
-    case 2: launch_stream_t<8, 12, P>(c, B, prm, mt, mp); break;
-    case 3: launch_stream_t<8, 16, P>(c, B, prm, mt, mp); break;
-    case 4: launch_stream_t<8, 24, P>(c, B, prm, mt, mp); break;
-    case 5: launch_stream_t<8, 32, P>(c, B, prm, mt, mp); break;
-    case 6: launch_stream_t<16, 16, P>(c, B, prm, mt, mp); break;
-    case 7: launch_stream_t<16, 20, P>(c, B, prm, mt, mp); break;
-    case 8: launch_stream_t<16, 24, P>(c, B, prm, mt, mp); break;
-    case 9: launch_stream_t<16, 32, P>(c, B, prm, mt, mp); break;
-    case 10: launch_stream_t<32, 16, P>(c, B, prm, mt, mp); break;
-    case 11: launch_stream_t<32, 20, P>(c, B, prm, mt, mp); break;
-    case 12: launch_stream_t<32, 24, P>(c, B, prm, mt, mp); break;
-    case 13: launch_stream_t<32, 32, P>(c, B, prm, mt, mp); break;
-    case 14: launch_stream_t<8, 20, P>(c, B, prm, mt, mp); break;
-    case 15: launch_stream_t<8, 28, P>(c, B, prm, mt, mp); break;
-    case 16: launch_stream_t<16, 28, P>(c, B, prm, mt, mp); break;
-    case 17: launch_stream_t<32, 28, P>(c, B, prm, mt, mp); break;
+    case 0: launch_stream_t<8, 4, P>(c, B, prm, mt, mp, lc); break;
+    case 1: launch_stream_t<8, 8, P>(c, B, prm, mt, mp, lc); break;
+    case 2: launch_stream_t<8, 12, P>(c, B, prm, mt, mp, lc); break;
+    case 3: launch_stream_t<8, 16, P>(c, B, prm, mt, mp, lc); break;
+    case 4: launch_stream_t<8, 24, P>(c, B, prm, mt, mp, lc); break;
+    case 5: launch_stream_t<8, 32, P>(c, B, prm, mt, mp, lc); break;
+    case 6: launch_stream_t<16, 16, P>(c, B, prm, mt, mp, lc); break;
+    case 7: launch_stream_t<16, 20, P>(c, B, prm, mt, mp, lc); break;
+    case 8: launch_stream_t<16, 24, P>(c, B, prm, mt, mp, lc); break;
+    case 9: launch_stream_t<16, 32, P>(c, B, prm, mt, mp, lc); break;
+    case 10: launch_stream_t<32, 16, P>(c, B, prm, mt, mp, lc); break;
+    case 11: launch_stream_t<32, 20, P>(c, B, prm, mt, mp, lc); break;
+    case 12: launch_stream_t<32, 24, P>(c, B, prm, mt, mp, lc); break;
+    case 13: launch_stream_t<32, 32, P>(c, B, prm, mt, mp, lc); break;
+    case 14: launch_stream_t<8, 20, P>(c, B, prm, mt, mp, lc); break;
+    case 15: launch_stream_t<8, 28, P>(c, B, prm, mt, mp, lc); break;
+    case 16: launch_stream_t<16, 28, P>(c, B, prm, mt, mp, lc); break;
+    case 17: launch_stream_t<32, 28, P>(c, B, prm, mt, mp, lc); break;
     default: fail(GPUSW_ERR_INVALID, "bad stream kernel shape");
   }
 }
@@ -775,6 +974,26 @@ int pick_stream_shape(int ncols, int ns, bool plain, const std::vector<double>* 
                                       kStreamShapes[i].cap()) * (*tuned)[i]
                            : stream_cost(kStreamShapes[i], ncols);
     if (best < 0 || cst < bc) {
+      best = i;
+      bc = cst;
+    }
+  }
+  return best;
+}
+
+// Latency form, for calls too small to fill the GPU (each CTA gets at most an item or two, so
+// the call lasts as long as its slowest item): an item's time is its passes x steps x the
+// instructions of one step, and a step costs about 5.5 W + 6 whatever G is (G lanes work in
+// parallel). So the shape of fewest passes x (5.5 W + 6), ties to the smaller team.
+int pick_stream_shape_latency(int ncols, int ns) {
+  int best = -1;
+  double bc = 0;
+  for (int i = 0; i < kNumStream; ++i) {
+    const Shape& sh = kStreamShapes[i];
+    if (profile_bytes(sh, ns) > kSmemCap) continue;
+    const int npass = (std::max(ncols, 1) + sh.cap() - 1) / sh.cap();
+    const double cst = (double)npass * (5.5 * sh.W + 6.0);
+    if (best < 0 || cst < bc || (cst == bc && sh.G < kStreamShapes[best].G)) {
       best = i;
       bc = cst;
     }
@@ -899,8 +1118,12 @@ void run_cross_stream(gpusw_ctx* c, Bufs& B, const Db& q, Db& r, const int32_t* 
   std::vector<std::vector<int>> bins(kNumStream);
   const int call_max = npairs ? *std::max_element(pair_cols.begin(), pair_cols.end()) : 0;
   const std::vector<double>* tuned = c->plain ? nullptr : find_tune(c, P);
+  // a call whose items cannot fill the GPU even in the narrowest teams' chunks is planned
+  // for latency (see pick_stream_shape_latency) instead of throughput
+  const bool latency = !c->plain && (long long)npairs * ((st.n_streams + 31) / 32) < 2ll * c->sms;
   for (int i = 0; i < npairs; ++i) {
-    const int sh = pick_stream_shape(c->plain ? call_max : pair_cols[i], h.ns, c->plain != 0, tuned);
+    const int sh = latency ? pick_stream_shape_latency(pair_cols[i], h.ns)
+                           : pick_stream_shape(c->plain ? call_max : pair_cols[i], h.ns, c->plain != 0, tuned);
     if (sh < 0) fail(GPUSW_ERR_SCHEME, "substitution table too large for the profile");
     bins[sh].push_back(i);
   }
@@ -944,15 +1167,16 @@ void run_cross_stream(gpusw_ctx* c, Bufs& B, const Db& q, Db& r, const int32_t* 
   sp.ovf = B.ovf.as<gsw::Ovf>(kOvfCap);
   sp.ovf_count = B.ovf_count.as<int>(1);
   sp.ovf_cap = kOvfCap;
-  int slot = 0;
-  for (const L& l : launches) {
-    sp.items = reinterpret_cast<const int2*>(dmeta + l.items_off);
-    sp.n_items = l.n_items;
-    sp.queue = reinterpret_cast<int*>(queues + slot++);
-    if (P == 2) launch_stream_shape<2>(c, B, l.shape, sp, st.max_total, l.multipass);
-    else launch_stream_shape<1>(c, B, l.shape, sp, st.max_total, l.multipass);
-  }
-  if (P == 2) launch_overflow_rescore(c, B, q, r, out, queues + slot++);
+  run_group(c, B, (int)launches.size(), [&](int i, const LaunchCfg& lc) {
+    const L& l = launches[i];
+    gsw::StreamParams lp = sp;
+    lp.items = reinterpret_cast<const int2*>(dmeta + l.items_off);
+    lp.n_items = l.n_items;
+    lp.queue = reinterpret_cast<int*>(queues + i);
+    if (P == 2) launch_stream_shape<2>(c, B, l.shape, lp, st.max_total, l.multipass, lc);
+    else launch_stream_shape<1>(c, B, l.shape, lp, st.max_total, l.multipass, lc);
+  });
+  if (P == 2) launch_overflow_rescore(c, B, q, r, out, queues + launches.size());
 }
 
 // Cross product of the queries `qlist` (a sublist of q) against every sequence of r into
@@ -1028,15 +1252,16 @@ void run_cross(gpusw_ctx* c, Bufs& B, const Db& q, const Db& r, const int32_t* q
   pp.ovf = B.ovf.as<gsw::Ovf>(kOvfCap);
   pp.ovf_count = B.ovf_count.as<int>(1);
   pp.ovf_cap = kOvfCap;
-  int slot = 0;
-  for (const PL& L : pl) {
-    pp.pairs = reinterpret_cast<const int2*>(dmeta + L.off_p);
-    pp.pair_out = reinterpret_cast<const int2*>(dmeta + L.off_o);
-    pp.n_items = (long long)L.n * nr;
-    pp.queue = queues + slot++;
-    launch_pairs(c, B, L.shape, P, local, pp, r.max_len, L.mcol > kPairShapes[L.shape].cap());
-  }
-  if (P == 2) launch_overflow_rescore(c, B, q, r, out, queues + slot++);
+  run_group(c, B, (int)pl.size(), [&](int i, const LaunchCfg& lc) {
+    const PL& L = pl[i];
+    gsw::PairsParams lp = pp;
+    lp.pairs = reinterpret_cast<const int2*>(dmeta + L.off_p);
+    lp.pair_out = reinterpret_cast<const int2*>(dmeta + L.off_o);
+    lp.n_items = (long long)L.n * nr;
+    lp.queue = queues + i;
+    launch_pairs(c, B, L.shape, P, local, lp, r.max_len, L.mcol > kPairShapes[L.shape].cap(), lc);
+  });
+  if (P == 2) launch_overflow_rescore(c, B, q, r, out, queues + pl.size());
 }
 
 // Largest number of int16 cells flagged by any one launch sequence of the call (read after
@@ -1318,6 +1543,17 @@ int gpusw_ctx_create(int device, gpusw_ctx** out) {
     CK(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     for (cudaEvent_t* e : {&c->ev0, &c->ev1, &c->ev2, &c->ev3}) CK(cudaEventCreate(e));
+    CK(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+    for (auto& z : c->zip) {
+      CK(cudaEventCreateWithFlags(&z.done, cudaEventDisableTiming));
+      z.B.set_held(&c->held);
+      z.image.held = &c->held;
+    }
+    c->zip_iota.held = &c->held;
+    for (int i = 0; i < kAuxStreams; ++i) {
+      CK(cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&c->join_ev[i], cudaEventDisableTiming));
+    }
   });
   if (rc != GPUSW_OK) {
     g_create_error = c->err;
@@ -1342,13 +1578,29 @@ void gpusw_ctx_destroy(gpusw_ctx* c) {
     cudaFree(d.base);
     cudaFree(d.order_base);
   }
+  for (int i = 0; i < kAuxStreams; ++i)
+    if (c->aux[i]) cudaStreamSynchronize(c->aux[i]);
+  for (auto& z : c->zip) {
+    if (z.pinned) cudaFreeHost(z.pinned);
+    if (z.pinned_out) cudaFreeHost(z.pinned_out);
+    for (cudaEvent_t e : z.tev)
+      if (e) cudaEventDestroy(e);
+    z.image.release();
+    z.B.release();
+    if (z.done) cudaEventDestroy(z.done);
+  }
+  c->zip_iota.release();
   c->plans.clear();
   c->shared.release();
   c->flush.release();
   if (c->pinned) cudaFreeHost(c->pinned);
   if (c->sub_d) cudaFree(c->sub_d);
-  for (cudaEvent_t e : {c->ev0, c->ev1, c->ev2, c->ev3})
+  for (cudaEvent_t e : {c->ev0, c->ev1, c->ev2, c->ev3, c->fork_ev})
     if (e) cudaEventDestroy(e);
+  for (int i = 0; i < kAuxStreams; ++i) {
+    if (c->join_ev[i]) cudaEventDestroy(c->join_ev[i]);
+    if (c->aux[i]) cudaStreamDestroy(c->aux[i]);
+  }
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -1533,6 +1785,169 @@ int gpusw_db_upload(gpusw_ctx* c, const uint8_t* codes, const int32_t* offsets, 
       throw;
     }
     tr.lap("copy");
+    c->held += d->bytes;
+    const int h = c->next_db++;
+    c->dbs[h] = std::move(d);
+    *out_db = h;
+  });
+}
+
+// ------------------------------------------------------------ packed images (persisted sets)
+// A packed set's image is the byte layout db_upload sends to the device: words (the packed
+// codes, every sequence 16-byte aligned, then 64 zero slack words) | int64 word offsets |
+// int32 lengths, each part starting on a 256-byte boundary.
+}  // extern "C"
+
+namespace {
+
+struct ImageLayout {
+  size_t words_b = 0, woff_o = 0, len_o = 0, image_b = 0;
+};
+
+ImageLayout image_layout(long long nwords, int n) {
+  ImageLayout L;
+  L.words_b = (size_t)(nwords + 64) * 4;
+  L.woff_o = (L.words_b + 255) & ~(size_t)255;
+  L.len_o = L.woff_o + (((size_t)std::max(1, n) * 8 + 255) & ~(size_t)255);
+  L.image_b = L.len_o + (size_t)std::max(1, n) * 4;
+  return L;
+}
+
+inline long long words_of(int len, int per) { return ((long long)(len + per - 1) / per + 3) & ~3ll; }
+
+}  // namespace
+
+extern "C" {
+
+int gpusw_pack_image(const uint8_t* codes, const int32_t* offsets, int32_t n, void* image,
+                     int64_t image_bytes, int64_t* out_need, int32_t* out_bits, int64_t* out_nwords) {
+  try {
+    if (!offsets || n < 0 || !out_need || !out_bits || !out_nwords)
+      fail(GPUSW_ERR_INVALID, "null offsets/outputs or negative count");
+    if (offsets[0] < 0) fail(GPUSW_ERR_INVALID, "offsets must be non-negative");
+    Db d;
+    d.n = n;
+    d.len.resize(n);
+    bool bad = false;
+    for (int i = 0; i < n; ++i) {
+      d.len[i] = offsets[i + 1] - offsets[i];
+      bad |= d.len[i] < 0;
+      d.max_len = std::max(d.max_len, d.len[i]);
+    }
+    if (bad) fail(GPUSW_ERR_INVALID, "offsets must be non-decreasing");
+    const long long total = n ? (long long)offsets[n] - offsets[0] : 0;
+    if (total > 0 && !codes) fail(GPUSW_ERR_INVALID, "null codes");
+    std::vector<int> tmax((size_t)host_threads() + 1, 0);
+    {
+      const uint8_t* b0 = codes ? codes + offsets[0] : nullptr;
+      std::atomic<int> slot{0};
+      parallel_ranges(total, [&](long long lo, long long hi) {
+        uint8_t m = 0;
+        for (long long k = lo; k < hi; ++k) m = std::max(m, b0[k]);
+        tmax[slot++] = m;
+      });
+    }
+    d.max_code = *std::max_element(tmax.begin(), tmax.end());
+    d.bits = d.max_code < 4 ? 2 : d.max_code < 16 ? 4 : d.max_code < 32 ? 5 : 8;
+    d.per = d.bits == 5 ? 6 : 32 / d.bits;
+    d.woff.resize(n);
+    long long w = 0;
+    for (int i = 0; i < n; ++i) {
+      d.woff[i] = w;
+      w += words_of(d.len[i], d.per);
+    }
+    const ImageLayout L = image_layout(w, n);
+    *out_need = (int64_t)L.image_b;
+    *out_bits = d.bits;
+    *out_nwords = w;
+    if (!image) return GPUSW_OK;  // sizing call
+    if (image_bytes < (int64_t)L.image_b) fail(GPUSW_ERR_MEMORY, "image buffer too small");
+    char* img = static_cast<char*>(image);
+    uint32_t* words = reinterpret_cast<uint32_t*>(img);
+    memset(img, 0, L.image_b);  // slack words and alignment gaps are zero in every image
+    parallel_ranges(n, [&](long long lo, long long hi) {
+      pack_range(codes, offsets, d, words, (int)lo, (int)hi);
+    });
+    if (n) {
+      memcpy(img + L.woff_o, d.woff.data(), (size_t)n * 8);
+      memcpy(img + L.len_o, d.len.data(), (size_t)n * 4);
+    }
+    return GPUSW_OK;
+  } catch (const Error& e) {
+    g_create_error = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_create_error = "host allocation failed";
+    return GPUSW_ERR_MEMORY;
+  }
+}
+
+int gpusw_db_upload_image(gpusw_ctx* c, const void* image, int64_t image_bytes, int32_t n,
+                          int32_t bits, int64_t nwords, int32_t* out_db) {
+  return guarded(c, [&] {
+    if (!image || !out_db || n < 0 || nwords < 0) fail(GPUSW_ERR_INVALID, "null image/handle or negative count");
+    if (bits != 2 && bits != 4 && bits != 5 && bits != 8) fail(GPUSW_ERR_INVALID, "bits must be 2, 4, 5 or 8");
+    const ImageLayout L = image_layout(nwords, n);
+    if ((size_t)image_bytes != L.image_b) fail(GPUSW_ERR_INVALID, "image size does not match its layout");
+    const char* img = static_cast<const char*>(image);
+    auto d = std::make_unique<Db>();
+    d->n = n;
+    d->bits = bits;
+    d->per = bits == 5 ? 6 : 32 / bits;
+    d->len.resize(n);
+    d->woff.resize(n);
+    if (n) {
+      memcpy(d->len.data(), img + L.len_o, (size_t)n * 4);
+      memcpy(d->woff.data(), img + L.woff_o, (size_t)n * 8);
+    }
+    // the image must describe itself consistently before any kernel reads it
+    long long w = 0;
+    for (int i = 0; i < n; ++i) {
+      if (d->len[i] < 0 || d->woff[i] != w) fail(GPUSW_ERR_INVALID, "corrupt image: offsets or lengths");
+      w += words_of(d->len[i], d->per);
+      d->max_len = std::max(d->max_len, d->len[i]);
+    }
+    if (w != nwords) fail(GPUSW_ERR_INVALID, "corrupt image: word count");
+    // largest code actually stored (threaded over sequences), checked against the scheme
+    // before scoring like an uploaded set's
+    const uint32_t* words = reinterpret_cast<const uint32_t*>(img);
+    const uint32_t mask = (1u << bits) - 1u;
+    std::vector<int> tmax((size_t)host_threads() + 1, 0);
+    std::atomic<int> slot{0};
+    parallel_ranges_min(n, 256, [&](long long lo, long long hi) {
+      uint32_t m = 0;
+      for (long long i = lo; i < hi; ++i) {
+        const uint32_t* sw = words + d->woff[i];
+        for (int cidx = 0; cidx < d->len[i]; ++cidx)
+          m = std::max(m, (sw[cidx / d->per] >> ((cidx % d->per) * bits)) & mask);
+      }
+      tmax[slot++] = (int)m;
+    });
+    d->max_code = *std::max_element(tmax.begin(), tmax.end());
+    set_device(c);
+    CK(cudaStreamSynchronize(c->stream));  // the staging buffer may still feed a copy
+    const size_t image_words = (L.image_b + 3) / 4;
+    if (image_words > c->pinned_words) {
+      if (c->pinned) cudaFreeHost(c->pinned);
+      c->pinned = nullptr;
+      c->pinned_words = 0;
+      CK(cudaMallocHost(&c->pinned, image_words * 4));
+      c->pinned_words = image_words;
+    }
+    char* stage = reinterpret_cast<char*>(c->pinned);
+    parallel_ranges(L.image_b, [&](long long lo, long long hi) { memcpy(stage + lo, img + lo, (size_t)(hi - lo)); });
+    CK(cudaMalloc(&d->base, L.image_b));
+    d->words = reinterpret_cast<uint32_t*>(d->base);
+    d->woff_d = reinterpret_cast<long long*>(static_cast<char*>(d->base) + L.woff_o);
+    d->len_d = reinterpret_cast<int*>(static_cast<char*>(d->base) + L.len_o);
+    d->bytes = (int64_t)L.image_b;
+    cudaError_t e = cudaMemcpyAsync(d->base, stage, L.image_b, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+      cudaFree(d->base);
+      d->base = nullptr;
+      fail(GPUSW_ERR_CUDA, std::string("image copy: ") + cudaGetErrorString(e));
+    }
     c->held += d->bytes;
     const int h = c->next_db++;
     c->dbs[h] = std::move(d);
@@ -1867,15 +2282,16 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
               pp.ovf = Bx.ovf.as<gsw::Ovf>(kOvfCap);
               pp.ovf_count = Bx.ovf_count.as<int>(1);
               pp.ovf_cap = kOvfCap;
-              int slot = 0;
-              for (const Bin& bn : plan_bins) {
-                pp.order = reinterpret_cast<const int*>(dm + o_ord) + bn.i0;
-                pp.n_align = bn.i1 - bn.i0;
-                pp.n_items = (pp.n_align + Pw - 1) / Pw;
-                pp.queue = queues + slot++;
-                launch_pairs(c, Bx, bn.shape, Pw, local, pp, bn.mrow, bn.mcol > kPairShapes[bn.shape].cap());
-              }
-              if (Pw == 2) launch_overflow_rescore(c, Bx, q, r, d_out, queues + slot++);
+              run_group(c, Bx, (int)plan_bins.size(), [&](int bi, const LaunchCfg& lc) {
+                const Bin& bn = plan_bins[bi];
+                gsw::PairsParams lp = pp;
+                lp.order = reinterpret_cast<const int*>(dm + o_ord) + bn.i0;
+                lp.n_align = bn.i1 - bn.i0;
+                lp.n_items = (lp.n_align + Pw - 1) / Pw;
+                lp.queue = queues + bi;
+                launch_pairs(c, Bx, bn.shape, Pw, local, lp, bn.mrow, bn.mcol > kPairShapes[bn.shape].cap(), lc);
+              });
+              if (Pw == 2) launch_overflow_rescore(c, Bx, q, r, d_out, queues + plan_bins.size());
             });
           };
         };
@@ -1899,6 +2315,464 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
     c->st.last_pairs = n;
     end_call(c);
     tr.lap("finish");
+  });
+}
+
+}  // extern "C"
+
+// ============================================================ zipped pairs, pipelined
+namespace {
+
+// One chunk of a zipped pair set: pairs [a, b) as two chunk-local packed sets, the launch
+// order (by shape, then row length descending) and its bins. Kept until the chunk's results
+// are read, so a chunk whose int16 overflow list filled up can be scored again in int32.
+struct ZipChunk {
+  long long a = 0, b = 0;
+  Db q, r;
+  std::vector<int> order;
+  std::vector<uint8_t> shp;
+  struct Bin { long long i0, i1; int shape, mrow, mcol; };
+  std::vector<Bin> bins;
+  size_t off_order = 0, image_bytes = 0;
+  int P = 2;
+  int bits_guess[2] = {2, 2};  // packing widths to try first (the previous chunk's)
+};
+
+constexpr long long kZipChunk = 1 << 17;  // pairs per pipeline chunk
+
+// Host half of a chunk, written into the slot's page-locked image (layout: q words | r words |
+// q woff | r woff | q len | r len | order, each 256-byte aligned), in two threaded passes over
+// the chunk's pairs: (1) lengths, kernel shapes (shape_of[length], or plain_shape), the
+// largest code of each side, word counts at every packing width, bin extents and whether the
+// input is already in launch order (by shape, row length descending); (2) word offsets, the
+// packed words of both sides and the metadata. Only a chunk that is out of order is sorted,
+// by a stable counting sort on one thread.
+void zip_prepare(gpusw_ctx* c, gpusw_ctx::ZipSlot& z, ZipChunk& ch, const uint8_t* qc,
+                 const int32_t* qo, const uint8_t* rc, const int32_t* ro,
+                 const std::vector<uint8_t>& shape_of, int big_shape, int plain_shape, HostTrace& tr) {
+  const int nc = (int)(ch.b - ch.a);
+  const HostScheme& h = c->sch;
+  Db* sets[2] = {&ch.q, &ch.r};
+  const uint8_t* codes[2] = {qc, rc};
+  const int32_t* offs[2] = {qo + ch.a, ro + ch.a};
+  for (Db* d : sets) {
+    d->n = nc;
+    d->len.resize(nc);
+    d->woff.resize(nc);
+  }
+  ch.shp.resize(nc);
+  constexpr int kPer[4] = {16, 8, 6, 4};  // codes per word at 2, 4, 5, 8 bits
+  struct P1 {
+    long long lo = 0, hi = 0;
+    int maxlen[2] = {0, 0};
+    long long words[2][4] = {};
+    int cnt[kNumPair] = {}, mrow[kNumPair] = {}, mcol[kNumPair] = {};
+    bool sorted = true;
+  };
+  const int nt = host_threads() + 1;
+  std::vector<P1> p1((size_t)nt);
+  std::atomic<int> slot{0};
+  auto before = [&](int i, int j) {  // pair j may follow pair i in launch order
+    const int si = ch.shp[i], sj = ch.shp[j];
+    return si < sj || (si == sj && std::min(ch.r.len[j], 65535) <= std::min(ch.r.len[i], 65535));
+  };
+  parallel_ranges_min(nc, 4096, [&](long long lo, long long hi) {
+    P1 pt;
+    pt.lo = lo;
+    pt.hi = hi;
+    for (int k = 0; k < 2; ++k) {
+      Db& d = *sets[k];
+      const int32_t* o = offs[k];
+      for (long long i = lo; i < hi; ++i) {
+        const int l = o[i + 1] - o[i];
+        d.len[i] = l;
+        pt.maxlen[k] = std::max(pt.maxlen[k], l);
+        for (int w = 0; w < 4; ++w) pt.words[k][w] += words_of(l, kPer[w]);
+      }
+    }
+    for (long long i = lo; i < hi; ++i) {
+      const int ql = ch.q.len[i], rl = ch.r.len[i];
+      const int sh = plain_shape >= 0 ? plain_shape : (ql < (int)shape_of.size() ? shape_of[ql] : big_shape);
+      ch.shp[i] = (uint8_t)sh;
+      pt.cnt[sh]++;
+      pt.mrow[sh] = std::max(pt.mrow[sh], rl);
+      pt.mcol[sh] = std::max(pt.mcol[sh], ql);
+      if (i > lo && !before((int)i - 1, (int)i)) pt.sorted = false;
+    }
+    p1[slot++] = pt;
+  });
+  const int used = slot.load();
+  std::sort(p1.begin(), p1.begin() + used, [](const P1& a, const P1& b) { return a.lo < b.lo; });
+  bool sorted = c->plain != 0;
+  int cnt[kNumPair] = {}, mrow[kNumPair] = {}, mcol[kNumPair] = {};
+  for (int t = 0; t < used; ++t) {
+    const P1& pt = p1[t];
+    if (!c->plain) {
+      sorted = (t == 0 ? true : sorted) && pt.sorted;
+      if (t > 0 && pt.hi > pt.lo && p1[t - 1].hi > p1[t - 1].lo && !before((int)p1[t - 1].hi - 1, (int)pt.lo))
+        sorted = false;
+    }
+    for (int k = 0; k < 2; ++k) sets[k]->max_len = std::max(t ? sets[k]->max_len : 0, pt.maxlen[k]);
+    for (int sh = 0; sh < kNumPair; ++sh) {
+      cnt[sh] += pt.cnt[sh];
+      mrow[sh] = std::max(mrow[sh], pt.mrow[sh]);
+      mcol[sh] = std::max(mcol[sh], pt.mcol[sh]);
+    }
+  }
+  if (nc == 0)
+    for (Db* d : sets) d->max_len = 0;
+  // packing widths: the guess (the previous chunk's widths), corrected after packing when the
+  // OR of the codes shows a wider one is needed (the chunk is then packed again)
+  long long wtotal[2];
+  std::vector<long long> wstart[2];
+  auto set_width = [&](int k, int bits) {
+    Db& d = *sets[k];
+    d.bits = bits;
+    d.per = bits == 5 ? 6 : 32 / bits;
+    const int widx = bits == 2 ? 0 : bits == 4 ? 1 : bits == 5 ? 2 : 3;
+    wstart[k].resize((size_t)used);
+    long long w = 0;
+    for (int t = 0; t < used; ++t) {
+      wstart[k][t] = w;
+      w += p1[t].words[k][widx];
+    }
+    wtotal[k] = w;
+  };
+  for (int k = 0; k < 2; ++k) set_width(k, ch.bits_guess[k]);
+  tr.lap("chunk: lengths, shapes");
+  // launch order and bins
+  ch.order.resize(nc);
+  const bool identity = sorted;
+  if (!identity) {  // stable counting sort on (shape, row length descending)
+    const int mm = std::min(ch.r.max_len, 65535);
+    auto key = [&](int i) { return (size_t)ch.shp[i] * (size_t)(mm + 1) + (size_t)(mm - std::min(ch.r.len[i], mm)); };
+    std::vector<int> bc((size_t)kNumPair * (mm + 1) + 1, 0);
+    for (int i = 0; i < nc; ++i) bc[key(i) + 1]++;
+    for (size_t k = 0; k + 1 < bc.size(); ++k) bc[k + 1] += bc[k];
+    for (int i = 0; i < nc; ++i) ch.order[bc[key(i)]++] = i;
+  }
+  ch.bins.clear();
+  long long i0 = 0;
+  for (int sh = 0; sh < kNumPair; ++sh) {
+    if (!cnt[sh]) continue;
+    ch.bins.push_back({i0, i0 + cnt[sh], sh, mrow[sh], mcol[sh]});
+    i0 += cnt[sh];
+  }
+  // image layout (it depends on the widths), then pass 2: word offsets, packed words and
+  // metadata, over the same ranges as pass 1, with the OR of each side's codes
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  size_t o_w[2], o_wo[2], o_l[2];
+  uint8_t side_or[2] = {0, 0};
+  auto pack_pass = [&]() {
+    const size_t words_b[2] = {(size_t)(wtotal[0] + 64) * 4, (size_t)(wtotal[1] + 64) * 4};
+    o_w[0] = 0;
+    o_w[1] = al(words_b[0]);
+    o_wo[0] = al(o_w[1] + words_b[1]);
+    o_wo[1] = al(o_wo[0] + (size_t)nc * 8);
+    o_l[0] = al(o_wo[1] + (size_t)nc * 8);
+    o_l[1] = al(o_l[0] + (size_t)nc * 4);
+    ch.off_order = al(o_l[1] + (size_t)nc * 4);
+    ch.image_bytes = ch.off_order + (size_t)std::max(nc, 1) * 4;
+    if (ch.image_bytes > z.pinned_bytes) {
+      if (z.pinned) cudaFreeHost(z.pinned);
+      z.pinned = nullptr;
+      z.pinned_bytes = 0;
+      const size_t want = ch.image_bytes + (ch.image_bytes >> 3);  // chunks differ a little
+      CK(cudaMallocHost(reinterpret_cast<void**>(&z.pinned), want));
+      z.pinned_bytes = want;
+    }
+    char* img = z.pinned;
+    for (int k = 0; k < 2; ++k) {
+      uint32_t* words = reinterpret_cast<uint32_t*>(img + o_w[k]);
+      std::fill(words + wtotal[k], words + wtotal[k] + 64, 0u);
+    }
+    std::vector<std::array<uint8_t, 2>> ors((size_t)nt, {0, 0});
+    std::atomic<int> oslot{0};
+    parallel_ranges_min(nc, 4096, [&](long long lo, long long hi) {
+      std::array<uint8_t, 2> o = {0, 0};
+      const int t = (int)(std::lower_bound(p1.begin(), p1.begin() + used, lo,
+                                           [](const P1& a, long long v) { return a.lo < v; }) - p1.begin());
+      for (int k = 0; k < 2; ++k) {
+        Db& d = *sets[k];
+        long long w = t < used && p1[t].lo == lo ? wstart[k][t] : 0;
+        if (!(t < used && p1[t].lo == lo))  // defensive: the split differs, recount
+          for (long long i = 0; i < lo; ++i) w += words_of(d.len[i], d.per);
+        for (long long i = lo; i < hi; ++i) {
+          d.woff[i] = w;
+          w += words_of(d.len[i], d.per);
+        }
+        pack_range(codes[k], offs[k], d, reinterpret_cast<uint32_t*>(img + o_w[k]), (int)lo, (int)hi, &o[k]);
+        memcpy(img + o_wo[k] + (size_t)lo * 8, d.woff.data() + lo, (size_t)(hi - lo) * 8);
+        memcpy(img + o_l[k] + (size_t)lo * 4, d.len.data() + lo, (size_t)(hi - lo) * 4);
+      }
+      int* ord = reinterpret_cast<int*>(img + ch.off_order);
+      if (identity)
+        for (long long i = lo; i < hi; ++i) ord[i] = (int)i;
+      else
+        memcpy(ord + lo, ch.order.data() + lo, (size_t)(hi - lo) * 4);
+      ors[oslot++] = o;
+    });
+    side_or[0] = side_or[1] = 0;
+    for (int x = 0; x < oslot.load(); ++x)
+      for (int k = 0; k < 2; ++k) side_or[k] |= ors[x][k];
+  };
+  pack_pass();
+  tr.lap("chunk: pack");
+  // the width each side needs (the OR has a bit at or above 2, 4 or 5 exactly when some code
+  // does); a side packed too narrow is packed again, and the next chunk starts from it
+  auto need_bits = [](uint8_t o) { return o < 4 ? 2 : o < 16 ? 4 : o < 32 ? 5 : 8; };
+  bool again = false;
+  for (int k = 0; k < 2; ++k) {
+    const int nb = sets[k]->bits == 8 ? 8 : need_bits(side_or[k]);
+    if (nb > sets[k]->bits) {
+      set_width(k, nb);
+      again = true;
+    }
+  }
+  if (again) pack_pass();
+  for (int k = 0; k < 2; ++k) {
+    Db& d = *sets[k];
+    ch.bits_guess[k] = d.bits;
+    // the codes must index the scheme's table: the OR bounds the largest code; at 8 bits (the
+    // whole words are copied, not ORed) or when the bound reaches the table, scan exactly
+    int mx = side_or[k];
+    if (d.bits == 8 || mx >= h.ns) {
+      const int32_t* o = offs[k];
+      const uint8_t* b0 = codes[k] + o[0];
+      std::vector<int> tmax((size_t)nt, 0);
+      std::atomic<int> sl{0};
+      parallel_ranges((long long)o[nc] - o[0], [&](long long lo, long long hi) {
+        uint8_t m = 0;
+        for (long long x = lo; x < hi; ++x) m = std::max(m, b0[x]);
+        tmax[sl++] = m;
+      });
+      mx = *std::max_element(tmax.begin(), tmax.end());
+    }
+    d.max_code = mx;
+    if (d.max_code >= h.ns) fail(GPUSW_ERR_INVALID, "sequence codes exceed the scheme's substitution table");
+  }
+  for (int k = 0; k < 2; ++k)  // the two passes agreed on the word layout
+    if (nc > 0 && sets[k]->woff[nc - 1] + words_of(sets[k]->len[nc - 1], sets[k]->per) != wtotal[k])
+      fail(GPUSW_ERR_CUDA, "internal error: packed chunk layout mismatch");
+  // device view of the image (filled by the slot's copy); grown with an eighth of headroom
+  if (ch.image_bytes > z.image.bytes) z.image.get(ch.image_bytes + (ch.image_bytes >> 3));
+  char* dimg = static_cast<char*>(z.image.p);
+  for (int k = 0; k < 2; ++k) {
+    Db& d = *sets[k];
+    d.words = reinterpret_cast<uint32_t*>(dimg + o_w[k]);
+    d.woff_d = reinterpret_cast<long long*>(dimg + o_wo[k]);
+    d.len_d = reinterpret_cast<int*>(dimg + o_l[k]);
+  }
+}
+
+// Device half of a chunk on stream st: the image copy (unless already resident), the
+// kernels of every bin, int16 overflow rescoring, and the copy of the scores (and of the
+// overflow count) into page-locked memory; then the slot's completion event.
+void zip_issue(gpusw_ctx* c, gpusw_ctx::ZipSlot& z, const ZipChunk& ch, int P, cudaStream_t st,
+               bool copy_image) {
+  const int nc = (int)(ch.b - ch.a);
+  const HostScheme& h = c->sch;
+  const bool local = h.mode == gsw::kModeLocal;
+  Bufs& B = z.B;
+  char* dimg = static_cast<char*>(z.image.p);
+  const bool tr = HostTrace::enabled();
+  if (tr && !z.tev[0])
+    for (cudaEvent_t& e : z.tev) CK(cudaEventCreate(&e));
+  if (tr) CK(cudaEventRecord(z.tev[0], st));
+  if (copy_image) CK(cudaMemcpyAsync(dimg, z.pinned, ch.image_bytes, cudaMemcpyHostToDevice, st));
+  if (tr) CK(cudaEventRecord(z.tev[1], st));
+  const int nslots = (int)ch.bins.size() + 2;
+  unsigned long long* queues = B.queue.as<unsigned long long>(nslots);
+  int* d_out = B.out.as<int>((size_t)nc);
+  int* ovf_flag = B.ovf_flag.as<int>(1);
+  gsw::PairsParams pp{};
+  pp.S = make_scheme(h, P);
+  pp.sub = c->sub_d;
+  pp.cols = ch.q.packed();
+  pp.rows = ch.r.packed();
+  pp.qi = static_cast<const int*>(c->zip_iota.p);
+  pp.rj = pp.qi;
+  pp.item_mode = 0;
+  pp.out = d_out;
+  pp.ovf = B.ovf.as<gsw::Ovf>(kOvfCap);
+  pp.ovf_count = B.ovf_count.as<int>(1);
+  pp.ovf_cap = kOvfCap;
+  const int* d_order = reinterpret_cast<const int*>(dimg + ch.off_order);
+  // strips of every launch side by side (a sizing pass first), all on this stream
+  const int nb = (int)ch.bins.size();
+  std::vector<long long> off((size_t)nb + 1, -1);
+  size_t total = 0;
+  auto bin_launch = [&](int bi, const LaunchCfg& lc) {
+    const ZipChunk::Bin& bn = ch.bins[bi];
+    gsw::PairsParams lp = pp;
+    lp.order = d_order + bn.i0;
+    lp.n_align = bn.i1 - bn.i0;
+    lp.n_items = (lp.n_align + P - 1) / P;
+    lp.queue = queues + bi;
+    launch_pairs(c, B, bn.shape, P, local, lp, bn.mrow, bn.mcol > kPairShapes[bn.shape].cap(), lc);
+  };
+  for (int bi = 0; bi <= nb; ++bi) {
+    size_t need = 0;
+    LaunchCfg sz;
+    sz.need = &need;
+    if (bi < nb) bin_launch(bi, sz);
+    else if (P == 2) launch_overflow_rescore(c, B, ch.q, ch.r, d_out, queues + nb, sz);
+    if (need) {
+      off[bi] = (long long)total;
+      total += need;
+    }
+  }
+  if (total) B.bnd.as<uint2>(total);
+  CK(cudaMemsetAsync(queues, 0, nslots * sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(ovf_flag, 0, sizeof(int), st));
+  if (P == 2) CK(cudaMemsetAsync(pp.ovf_count, 0, sizeof(int), st));
+  for (int bi = 0; bi < nb; ++bi) {
+    LaunchCfg lc;
+    lc.st = st;
+    lc.bnd_off = off[bi];
+    bin_launch(bi, lc);
+  }
+  if (P == 2) {
+    LaunchCfg lc;
+    lc.st = st;
+    lc.bnd_off = off[nb];
+    launch_overflow_rescore(c, B, ch.q, ch.r, d_out, queues + nb, lc);
+  }
+  if (tr) CK(cudaEventRecord(z.tev[2], st));
+  CK(cudaMemcpyAsync(z.pinned_out, d_out, (size_t)nc * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(z.pinned_out + nc, ovf_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (tr) CK(cudaEventRecord(z.tev[3], st));
+  CK(cudaEventRecord(z.done, st));
+}
+
+}  // namespace
+
+extern "C" {
+
+int gpusw_score_pairs_zip(gpusw_ctx* c, const uint8_t* q_codes, const int32_t* q_offsets,
+                          const uint8_t* r_codes, const int32_t* r_offsets, int64_t n, int dtype,
+                          int32_t* out) {
+  constexpr int kSlots = 3;  // chunks in flight: the host packs one while two are on the GPU
+  cudaStream_t streams[kSlots] = {c ? c->stream : nullptr, c ? c->aux[0] : nullptr, c ? c->aux[1] : nullptr};
+  return guarded(c, [&] {
+    if (!c->has_scheme) fail(GPUSW_ERR_SCHEME, "no scheme set (call gpusw_set_scheme first)");
+    if (n < 0 || (n > 0 && (!q_offsets || !r_offsets || !out))) fail(GPUSW_ERR_INVALID, "null arrays or negative count");
+    if (n >= (1ll << 31)) fail(GPUSW_ERR_INVALID, "at most 2^31 - 1 pairs per call");
+    if (n > 0 && (q_offsets[0] < 0 || r_offsets[0] < 0)) fail(GPUSW_ERR_INVALID, "offsets must be non-negative");
+    HostTrace tr("score_pairs_zip");
+    // lengths of every pair: validation, extents and cells (threaded)
+    int max_n = 0, max_m = 0;
+    double cells = 0;
+    {
+      struct Part { int mn = 0, mm = 0; double cells = 0; bool bad = false; };
+      std::vector<Part> part((size_t)host_threads() + 1);
+      std::atomic<int> slot{0};
+      parallel_ranges(n, [&](long long lo, long long hi) {
+        Part pt;
+        for (long long i = lo; i < hi; ++i) {
+          const int ql = q_offsets[i + 1] - q_offsets[i], rl = r_offsets[i + 1] - r_offsets[i];
+          pt.bad |= ql < 0 || rl < 0;
+          pt.mn = std::max(pt.mn, ql);
+          pt.mm = std::max(pt.mm, rl);
+          pt.cells += (double)ql * rl;
+        }
+        part[slot++] = pt;
+      });
+      for (const Part& pt : part) {
+        if (pt.bad) fail(GPUSW_ERR_INVALID, "offsets must be non-decreasing");
+        max_n = std::max(max_n, pt.mn);
+        max_m = std::max(max_m, pt.mm);
+        cells += pt.cells;
+      }
+    }
+    if (n > 0 && ((q_offsets[n] > q_offsets[0] && !q_codes) || (r_offsets[n] > r_offsets[0] && !r_codes)))
+      fail(GPUSW_ERR_INVALID, "null codes");
+    begin_call(c);
+    c->last_bufs = nullptr;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    const int P = n > 0 ? choose_width(c, dtype, max_n, max_m) : 1;
+    const long long chunk = std::min<long long>(kZipChunk, std::max<long long>(1, n));
+    if (n > 0 && c->zip_iota_n < chunk) {
+      std::vector<int> io((size_t)chunk);
+      std::iota(io.begin(), io.end(), 0);
+      CK(cudaMemcpy(c->zip_iota.get((size_t)chunk * 4), io.data(), (size_t)chunk * 4, cudaMemcpyHostToDevice));
+      c->zip_iota_n = chunk;
+    }
+    // kernel shape of every column length up to 4,096 (longer ones: the widest shape)
+    std::vector<uint8_t> shape_of(4097);
+    for (int L = 0; L <= 4096; ++L) shape_of[L] = (uint8_t)pick_pair_shape(std::max(1, L), c->sch.ns);
+    const int big_shape = pick_pair_shape(1 << 30, c->sch.ns);
+    const int plain_shape = c->plain ? pick_pair_shape(std::max(1, max_n), c->sch.ns) : -1;
+    tr.lap("validate");
+    ZipChunk chs[kSlots];
+    const long long K = (n + chunk - 1) / chunk;
+    const int used_slots = (int)std::min<long long>(kSlots, std::max(1ll, K));
+    if (used_slots > 1) {  // the other streams start after the work already on the first
+      CK(cudaEventRecord(c->fork_ev, c->stream));
+      for (int sl = 1; sl < used_slots; ++sl) CK(cudaStreamWaitEvent(streams[sl], c->fork_ev, 0));
+    }
+    // results of the chunk in slot s: copied out, or scored again in int32 if its overflow
+    // list was full
+    auto finish = [&](int sl) {
+      gpusw_ctx::ZipSlot& z = c->zip[sl];
+      ZipChunk& ch = chs[sl];
+      CK(cudaEventSynchronize(z.done));
+      const int nc = (int)(ch.b - ch.a);
+      if (HostTrace::enabled() && z.tev[0]) {
+        float a = 0, b = 0, d = 0, g = 0;
+        cudaEventElapsedTime(&a, z.tev[0], z.tev[1]);
+        cudaEventElapsedTime(&b, z.tev[1], z.tev[2]);
+        cudaEventElapsedTime(&d, z.tev[2], z.tev[3]);
+        cudaEventElapsedTime(&g, c->ev1, z.tev[0]);
+        std::fprintf(stderr, "[gpusw] zip chunk %lld slot %d: starts %.3f ms after the call, copy in %.3f, kernels %.3f, copy out %.3f ms\n",
+                     ch.a / kZipChunk, sl, g, a, b, d);
+      }
+      if (ch.P == 2 && z.pinned_out[nc] > kOvfCap) {
+        ch.P = 1;
+        zip_issue(c, z, ch, 1, streams[sl], false);
+        CK(cudaEventSynchronize(z.done));
+      }
+      c->st.last_overflow = std::max<int64_t>(c->st.last_overflow, z.pinned_out[nc]);
+      memcpy(out + ch.a, z.pinned_out, (size_t)nc * 4);
+    };
+    try {
+      for (long long k = 0; k < K; ++k) {
+        const int sl = (int)(k % kSlots);
+        gpusw_ctx::ZipSlot& z = c->zip[sl];
+        if (k >= kSlots) finish(sl);
+        tr.lap("chunk: wait for the slot");
+        ZipChunk& ch = chs[sl];
+        ch.a = k * chunk;
+        ch.b = std::min<long long>(n, ch.a + chunk);
+        ch.P = P;
+        const size_t nc = (size_t)(ch.b - ch.a);
+        if (nc + 1 > z.pinned_out_n) {
+          if (z.pinned_out) cudaFreeHost(z.pinned_out);
+          z.pinned_out = nullptr;
+          z.pinned_out_n = 0;
+          CK(cudaMallocHost(reinterpret_cast<void**>(&z.pinned_out), (nc + 1) * 4));
+          z.pinned_out_n = nc + 1;
+        }
+        zip_prepare(c, z, ch, q_codes, q_offsets, r_codes, r_offsets, shape_of, big_shape, plain_shape, tr);
+        tr.lap("chunk: checks");
+        zip_issue(c, z, ch, P, streams[sl], true);
+        tr.lap("chunk: issue");
+      }
+      for (long long k = std::max(0ll, K - kSlots); k < K; ++k) finish((int)(k % kSlots));
+    } catch (...) {
+      for (cudaStream_t st : streams) cudaStreamSynchronize(st);
+      throw;
+    }
+    tr.lap("pipeline");
+    for (int sl = 1; sl < used_slots; ++sl) {
+      CK(cudaEventRecord(c->join_ev[sl - 1], streams[sl]));
+      CK(cudaStreamWaitEvent(c->stream, c->join_ev[sl - 1], 0));
+    }
+    CK(cudaEventRecord(c->ev2, c->stream));
+    CK(cudaEventRecord(c->ev3, c->stream));
+    c->st.last_cells = cells;
+    c->st.last_pairs = n;
+    end_call(c);
   });
 }
 

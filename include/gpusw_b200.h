@@ -98,6 +98,26 @@ int gpusw_set_scheme(gpusw_ctx *ctx, int mode, int gap_open, int gap_extend, int
 int gpusw_db_upload(gpusw_ctx *ctx, const uint8_t *codes, const int32_t *offsets, int32_t n,
                     int32_t *out_db);
 
+/* Packed image of an encoded set, for storing it (host only, no GPU): the exact byte
+ * layout gpusw_db_upload sends to the device -- packed words (every sequence 16-byte
+ * aligned, then 64 zero slack words) | int64 word offsets | int32 lengths, each part on a
+ * 256-byte boundary. With image == NULL only *out_need (bytes), *out_bits and *out_nwords
+ * (packed words without the slack) are set; otherwise image_bytes must be at least
+ * *out_need. Errors set gpusw_last_error(NULL). Replaces the per-process re-encoding of a
+ * reference set (src/gpusw/aligner.py:69-77, src/gpusw/encode.py:204-215): a set packed
+ * once is stored and uploaded as is by gpusw_db_upload_image. */
+int gpusw_pack_image(const uint8_t *codes, const int32_t *offsets, int32_t n, void *image,
+                     int64_t image_bytes, int64_t *out_need, int32_t *out_bits,
+                     int64_t *out_nwords);
+
+/* Upload a packed image made by gpusw_pack_image (n sequences, `bits` per residue,
+ * nwords packed words) without packing it again. The image is checked before it is used:
+ * its size, word offsets and lengths must agree, and its largest stored code is found
+ * (and checked against the scheme at scoring time, as for gpusw_db_upload). Same handle
+ * semantics as gpusw_db_upload. */
+int gpusw_db_upload_image(gpusw_ctx *ctx, const void *image, int64_t image_bytes, int32_t n,
+                          int32_t bits, int64_t nwords, int32_t *out_db);
+
 /* Release a sequence set. */
 int gpusw_db_free(gpusw_ctx *ctx, int32_t db);
 
@@ -124,6 +144,21 @@ int gpusw_topk(gpusw_ctx *ctx, int32_t qdb, int32_t rdb, const int32_t *qlist, i
  * src/gpusw/kernel.py:178-190. */
 int gpusw_score_pairs(gpusw_ctx *ctx, int32_t qdb, int32_t rdb, const int32_t *qi,
                       const int32_t *rj, int64_t n, int dtype, int32_t *out);
+
+/* Zipped pairs from host buffers in one call: out[i] = score(query i, reference i) for
+ * i < n, with query i at q_codes[q_offsets[i] .. q_offsets[i + 1]) and reference i at
+ * r_codes[r_offsets[i] .. r_offsets[i + 1]) (code bytes, int32 offsets of n + 1 entries,
+ * the reference package's Encoded layout). Equal to gpusw_db_upload of both sets followed
+ * by gpusw_score_pairs with qi = rj = 0..n-1, but pipelined: chunks of 131,072 pairs are
+ * packed on the host while the GPU scores the previous chunk, on two streams, so host
+ * packing, copies and kernels overlap; nothing stays resident after the call. Replaces
+ * src/gpusw/__init__.py:145-189 (align_pairs with pairs=None) with its
+ * src/gpusw/aligner.py:69-87 uploads and src/gpusw/backends/cuda.py:68-85 (run_pairs).
+ * On an error (decreasing offsets, a code >= the scheme's table side) out[] is
+ * unspecified. */
+int gpusw_score_pairs_zip(gpusw_ctx *ctx, const uint8_t *q_codes, const int32_t *q_offsets,
+                          const uint8_t *r_codes, const int32_t *r_offsets, int64_t n,
+                          int dtype, int32_t *out);
 
 /* Best-cell coordinates of explicit pairs (int32): for every pair, out_score receives the
  * maximum of H over all cells and out_rend/out_qend the 0-based reference row and query

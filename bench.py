@@ -387,6 +387,15 @@ def packed_bytes(offs: np.ndarray, bits: int) -> int:
     return int(words.sum() * 4 + 64 * 4 + lens.shape[0] * 20)
 
 
+def hbm_peak():
+    """Measured HBM copy bandwidth (GB/s) of this pool's B200s, and where it came from."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback 6.65 TB/s (earlier measurement on this pool)"
+
+
 def roofline(cells, score_ms, dpx, wl=None, bits=None):
     """Scoring kernels against the per-pipe instruction ceilings (GCUPS)."""
     alu = dpx * 2.0 / ALU_OPS_PER_REG / 1e9
@@ -525,6 +534,12 @@ def measure(ctx, group, world, local, wl, *, steps, warmup, plain_steps, e2e_ste
            "config": config_of(wl)}
     rec["roofline"]["kernel_ms_per_step"] = sum(score_ms) / steps
     rec["roofline"]["topk_ms_per_step"] = sum(topk_ms) / steps
+    if wl.k and sum(topk_ms) > 0:  # the top-k stage reads the int32 score block once: HBM-bound
+        gbs = wl.nq * wl.nr * 4 / (sum(topk_ms) / steps * 1e-3) / 1e9
+        peak, src = hbm_peak()
+        rec["roofline"]["topk_stage"] = {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                         "frac": gbs / peak, "peak_source": src,
+                                         "bytes_per_step": wl.nq * wl.nr * 4}
 
     # CPU baselines and bit-exact checks of their samples (rank 0, N = 1)
     rank = int(os.environ.get("RANK", 0))

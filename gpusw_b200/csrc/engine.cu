@@ -738,6 +738,15 @@ struct Staging {
   }
 };
 
+// Top-k of nrows score rows of ncols (row stride ncols) into (nrows, kk) outputs: the
+// threshold-and-filter kernel up to 32, the multi-round kernel beyond.
+void launch_topk(const int* d_scores, int nrows, int ncols, int kk, int* d_idx, int* d_sc, cudaStream_t st) {
+  if (nrows <= 0 || kk <= 0) return;
+  if (kk <= 32) gsw::topk_filter_kernel<<<nrows, 256, 0, st>>>(d_scores, ncols, ncols, kk, d_idx, d_sc, kk);
+  else gsw::topk_kernel<<<nrows, 256, 0, st>>>(d_scores, ncols, ncols, kk, d_idx, d_sc, kk);
+  CK(cudaGetLastError());
+}
+
 // Runs the n shape launches of one call, launch(i, cfg) issuing (or, with cfg.need set,
 // sizing) launch i. A first pass sizes the multi-pass boundary strips of every launch and
 // places them side by side in one allocation; then the launches go out round-robin on the
@@ -2065,9 +2074,7 @@ int gpusw_topk(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qlist, int
             const int nb = std::min(qb, nq - b0);
             staged(c, B, false, [&] { run_cross(c, B, q, r, qlist + b0, nb, Pw, d_out, r.n); });
             staged(c, B, true, [&] {
-              gsw::topk_kernel<<<nb, 256, 0, c->stream>>>(d_out, r.n, r.n, kk, d_idx + (size_t)b0 * kk,
-                                                           d_sc + (size_t)b0 * kk, kk);
-              CK(cudaGetLastError());
+              launch_topk(d_out, nb, r.n, kk, d_idx + (size_t)b0 * kk, d_sc + (size_t)b0 * kk, c->stream);
               c->st.last_launches++;
             });
             if (c->plain && !B.capturing) {  // one batch per call: results back per batch

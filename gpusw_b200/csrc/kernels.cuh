@@ -395,6 +395,123 @@ __global__ void __launch_bounds__(256) topk_kernel(const int* __restrict__ score
 }
 
 
+// Per-row top-k for k <= 32 by threshold and filter, one CTA (256 threads) per row:
+//  1. each thread takes the largest score of its strided part of the row; the k-th largest of
+//     these 256 maxima, T, is a lower bound of the row's k-th score (the k threads holding
+//     the larger maxima hold k distinct scores >= T);
+//  2. a second pass over the row (now mostly in L2) appends every (score >= T, index) to a
+//     shared candidate list -- it holds the whole top-k, since every top-k score is >= T;
+//  3. the candidates are ranked by (score desc, index asc), each by counting the candidates
+//     that beat it, and the first k written.
+// A row with more than kTopkCand candidates (massive ties at T) falls back to k rounds of
+// block-wide arg-max over the whole row. Same keys, same order as topk_kernel.
+constexpr int kTopkCand = 2048;
+
+__device__ __forceinline__ int topk_kth_of_block(int v, int k, int* s_tmp) {
+  // k-th largest of the 256 values v (one per thread): each thread counts how many values
+  // beat its own (ties broken by thread index) and the one with rank k - 1 publishes it
+  const int t = threadIdx.x;
+  s_tmp[t] = v;
+  __syncthreads();
+  int rank = 0;
+  for (int i = 0; i < 256; ++i) {
+    const int o = s_tmp[i];
+    rank += (o > v) || (o == v && i < t);
+  }
+  __syncthreads();
+  if (rank == k - 1) s_tmp[256] = v;
+  __syncthreads();
+  return s_tmp[256];
+}
+
+__global__ void __launch_bounds__(256) topk_filter_kernel(const int* __restrict__ scores, long long ld,
+                                                          int ncols, int k, int* out_idx,
+                                                          int* out_score, long long out_ld) {
+  __shared__ int s_tmp[257];
+  __shared__ int s_n;
+  __shared__ int s_sc[kTopkCand];
+  __shared__ int s_ix[kTopkCand];
+  const int row = blockIdx.x;
+  const int* srow = scores + (long long)row * ld;
+  const int kk = min(k, ncols);
+  const bool vec = (ld & 3) == 0;
+  const int n4 = vec ? ncols / 4 : 0;
+  // pass 1: per-thread maximum
+  int m = INT_MIN;
+  for (int q = threadIdx.x; q < n4; q += 256) {
+    const int4 x = __ldg(reinterpret_cast<const int4*>(srow) + q);
+    m = max(m, max(max(x.x, x.y), max(x.z, x.w)));
+  }
+  for (int j = 4 * n4 + threadIdx.x; j < ncols; j += 256) m = max(m, __ldg(srow + j));
+  // threads without elements hold INT_MIN, which never raises T above a real score
+  const int T = topk_kth_of_block(m, min(kk, 256), s_tmp);
+  if (threadIdx.x == 0) s_n = 0;
+  __syncthreads();
+  // pass 2: candidates >= T
+  auto add = [&](int sc, int j) {
+    if (sc < T) return;
+    const int p = atomicAdd(&s_n, 1);
+    if (p < kTopkCand) {
+      s_sc[p] = sc;
+      s_ix[p] = j;
+    }
+  };
+  for (int q = threadIdx.x; q < n4; q += 256) {
+    const int4 x = __ldg(reinterpret_cast<const int4*>(srow) + q);
+    if (max(max(x.x, x.y), max(x.z, x.w)) < T) continue;
+    add(x.x, 4 * q);
+    add(x.y, 4 * q + 1);
+    add(x.z, 4 * q + 2);
+    add(x.w, 4 * q + 3);
+  }
+  for (int j = 4 * n4 + threadIdx.x; j < ncols; j += 256) add(__ldg(srow + j), j);
+  __syncthreads();
+  const int nc = s_n;
+  if (nc <= kTopkCand) {
+    // 3: rank every candidate among the candidates; ranks < kk are the output positions
+    for (int c = threadIdx.x; c < nc; c += 256) {
+      const int sc = s_sc[c], ix = s_ix[c];
+      int rank = 0;
+      for (int o = 0; o < nc && rank < kk; ++o) {
+        const int so = s_sc[o];
+        rank += (so > sc) || (so == sc && s_ix[o] < ix);
+      }
+      if (rank < kk) {
+        out_idx[(long long)row * out_ld + rank] = ix;
+        out_score[(long long)row * out_ld + rank] = sc;
+      }
+    }
+    return;
+  }
+  // too many ties at T: kk rounds of block-wide arg-max over the row, each below the last
+  // round's key (few registers; only rows with massive ties come here)
+  unsigned long long bound = ~0ull;
+  for (int s = 0; s < kk; ++s) {
+    unsigned long long best = 0ull;
+    for (int j = threadIdx.x; j < ncols; j += 256) {
+      const unsigned long long key = topk_key(__ldg(srow + j), j);
+      if (key < bound && key > best) best = key;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const unsigned long long o = __shfl_xor_sync(0xFFFFFFFFu, best, off);
+      best = o > best ? o : best;
+    }
+    __shared__ unsigned long long s_best[8];
+    if ((threadIdx.x & 31) == 0) s_best[threadIdx.x / 32] = best;
+    __syncthreads();
+    best = s_best[0];
+#pragma unroll
+    for (int w = 1; w < 8; ++w) best = s_best[w] > best ? s_best[w] : best;
+    if (threadIdx.x == 0) {
+      out_idx[(long long)row * out_ld + s] = (int)(~(unsigned)(best & 0xFFFFFFFFull));
+      out_score[(long long)row * out_ld + s] = (int)((unsigned)(best >> 32) ^ 0x80000000u);
+    }
+    bound = best;
+    __syncthreads();
+  }
+}
+
 // -------------------------------------------------------------------------------------
 // Local-mode cross product over row *streams*: rows (sorted longest first) are grouped
 // in streams of kStreamRows; a work item is (column pair, chunk of nteams streams); each

@@ -166,7 +166,7 @@ void slot_launch(gpusw_server* s, Slot& sl, int P) {
   int* d_idx = B.idx.as<int>((size_t)nq * kk);
   int* d_sc = B.sc.as<int>((size_t)nq * kk);
   run_cross(c, B, sl.q, *s->refs, qlist.data(), nq, P, d_out, nr);
-  gsw::topk_kernel<<<nq, 256, 0, c->stream>>>(d_out, nr, nr, kk, d_idx, d_sc, kk);
+  launch_topk(d_out, nq, nr, kk, d_idx, d_sc, c->stream);
   CK(cudaGetLastError());
   const size_t need = (size_t)nq * kk;
   if (need > sl.h_cap) {

@@ -32,12 +32,15 @@ def test_top_k_matches_full_sort():
     assert tk.scores is None and tk.topk_idx.shape == (3, 2)
 
 
-@pytest.mark.parametrize("k", [1, 5, 31, 32, 33, 70, 400])
-def test_top_k_tie_order_any_k(k):
-    """Many ties (short, low-entropy sequences): order must be (score desc, index asc)."""
-    rng = np.random.default_rng(k)
+@pytest.mark.parametrize("k", [1, 5, 8, 9, 16, 17, 31, 32, 33, 70, 400])
+@pytest.mark.parametrize("nr", [300, 301, 2003])
+def test_top_k_tie_order_any_k(k, nr):
+    """Many ties (short, low-entropy sequences): order must be (score desc, index asc), for
+    every list depth of the one-pass kernel (k <= 8, 16, 32), the multi-round kernel beyond,
+    and rows whose length is not a multiple of four (the scalar tail of the 128-bit loads)."""
+    rng = np.random.default_rng(k * 7 + nr)
     qs = rand_seqs(rng, 7, 1, 12, "AC")
-    rs = rand_seqs(rng, 300, 0, 12, "AC")
+    rs = rand_seqs(rng, nr, 0, 12, "AC")
     al = Aligner("dna").index(rs).set_queries(qs)
     tk = al.top_k(k=k)
     full = al.score_cross()

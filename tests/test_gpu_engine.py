@@ -128,3 +128,50 @@ def test_autotune_table_and_results_unchanged():
         assert np.array_equal(al.score_cross().astype(np.int64), want)
     finally:
         ctx.set_options()
+
+
+@pytest.mark.parametrize("name,alpha", [("dna", "ACGT"), ("blosum62", "ARNDCQEGHILKMFPSTWYV")])
+def test_overlapping_shape_launches_with_multipass(name, alpha):
+    """A call whose query pairs span many streaming-kernel shapes, several of them multi-pass
+    (columns beyond 1,024), with enough references to be planned for throughput: its shape
+    launches run on several streams at once, each multi-pass launch with its own boundary
+    strips. Scores and top-k equal the oracle eagerly, on the recording call and on replay."""
+    sch = Scheme.preset(name)
+    rng = np.random.default_rng(71)
+    qs = rand_seqs(rng, 40, 10, 2600, alpha)
+    rs = rand_seqs(rng, 4000, 20, 600, alpha)
+    al = Aligner(sch).index(rs).set_queries(qs)
+    want = oracle.score_cross(funnel(qs, sch), funnel(rs, sch), sch)
+    idx, sc = oracle.topk_stable(want, 7)
+    for _ in range(3):  # eager, eager + recorded, graph replay
+        assert np.array_equal(al.score_cross().astype(np.int64), want)
+        tk = al.top_k(k=7)
+        assert np.array_equal(tk.topk_idx, idx) and np.array_equal(tk.topk_scores, sc)
+    assert al._ctx().stats().last_launches >= 3
+
+
+def test_small_calls_latency_shapes():
+    """Calls too small to fill the GPU take the latency-planned shapes (few passes of narrow
+    register strips): every column length, including multi-pass ones, stays exact."""
+    rng = np.random.default_rng(72)
+    for lo, hi, nq, nr in [(1, 90, 5, 7), (80, 200, 32, 128), (900, 2300, 3, 9)]:
+        qs = rand_seqs(rng, nq, lo, hi, "ACGT")
+        rs = rand_seqs(rng, nr, lo, hi, "ACGT")
+        for dtype in ("auto", "int32"):
+            sch = schemes.DNA.replace(dtype=dtype)
+            got = Aligner(sch).index(rs).set_queries(qs).score_cross()
+            want = oracle.score_cross(funnel(qs, sch), funnel(rs, sch), sch)
+            assert np.array_equal(got.astype(np.int64), want)
+
+
+def test_global_cross_multi_shape_bins():
+    """Global and semiglobal cross products run on the pairs kernel in cross mode: pairs of
+    many column lengths land in several bins (one multi-pass) whose launches overlap."""
+    rng = np.random.default_rng(73)
+    qs = rand_seqs(rng, 24, 5, 1300, "ACGT")
+    rs = rand_seqs(rng, 150, 5, 700, "ACGT")
+    for sch in (schemes.DNA.replace(mode="global"), schemes.DNA_SEMIGLOBAL):
+        al = Aligner(sch).index(rs).set_queries(qs)
+        want = oracle.score_cross(funnel(qs, sch), funnel(rs, sch), sch)
+        for _ in range(3):
+            assert np.array_equal(al.score_cross().astype(np.int64), want)

@@ -219,12 +219,21 @@ __global__ void __launch_bounds__(256, P8 ? 2 : 1) pairs_kernel(const PairsParam
     n_items = min(*p.ovf_in_count, p.ovf_in_cap);
     if (blockIdx.x == 0 && threadIdx.x == 0 && p.ovf_flag) atomicMax(p.ovf_flag, *p.ovf_in_count);
   }
+  // The next work item is taken from the queue and decoded (order -> pair indices) at the
+  // top of the current one, so that chain of dependent global loads completes while this item
+  // is scored instead of stalling the team between items (10^6 read/window pairs: +6.5 %).
+  unsigned long long tq = 0;
+  if (lane == 0) tq = atomicAdd(p.queue, 1ull);
+  long long t_next = (long long)__shfl_sync(wmask, tq, 0, G);
+  PairItem<P> it_next{};
+  if (t_next < n_items) it_next = decode_item<P>(p, t_next);
   for (;;) {
-    unsigned long long t = 0;
-    if (lane == 0) t = atomicAdd(p.queue, 1ull);
-    t = __shfl_sync(wmask, t, 0, G);
-    if ((long long)t >= n_items) break;
-    const PairItem<P> it = decode_item<P>(p, (long long)t);
+    const long long t = t_next;
+    if (t >= n_items) break;
+    const PairItem<P> it = it_next;
+    if (lane == 0) tq = atomicAdd(p.queue, 1ull);
+    t_next = (long long)__shfl_sync(wmask, tq, 0, G);
+    if (t_next < n_items) it_next = decode_item<P>(p, t_next);
     int n[P], m[P];
 #pragma unroll
     for (int a = 0; a < P; ++a) {

@@ -41,6 +41,7 @@ class Stats(ctypes.Structure):
         ("total_launches", ctypes.c_int64),
         ("total_overflow", ctypes.c_int64),
         ("device_bytes", ctypes.c_int64),
+        ("last_inter_items", ctypes.c_int64),
     ]
 
 
@@ -311,8 +312,9 @@ class Context:
                     pass
 
     def set_options(self, plain: bool = False, mem_budget: int = 0, autotune: bool = True,
-                    graphs: bool = True) -> None:
-        flags = (0 if autotune else 1) | (0 if graphs else 2)
+                    graphs: bool = True, one_launch: bool = False, inter: bool = True) -> None:
+        flags = ((0 if autotune else 1) | (0 if graphs else 2) | (4 if one_launch else 0)
+                 | (0 if inter else 8))
         self._check(self.lib.gpusw_set_options(self.handle, int(bool(plain)), int(mem_budget), flags))
 
     def autotune(self, width: int = 2) -> list[float]:

@@ -118,6 +118,7 @@ struct Db {
     int8_t* bytes = nullptr;
     long long* off = nullptr;
     int* total = nullptr;
+    std::vector<int> total_h;  // host copy of the totals (item costs of a multi-shape launch)
     int n_streams = 0, max_total = 0;
     int64_t nbytes = 0;
   };
@@ -167,6 +168,7 @@ size_t profile_bytes(const Shape& s, int ns) { return (size_t)(ns + 1) * pstride
 // captured CUDA graph keeps the raw pointers.
 struct Bufs {
   DevBuf meta, queue, ovf, ovf_count, ovf_flag, bnd, out, idx, sc;
+  long long inter_items = 0;  // items of the inter-sequence pairs kernel in this launch sequence
   std::vector<cudaEvent_t> pool;
   int pool_used = 0;
   std::vector<std::pair<int, int>> score_marks, topk_marks;
@@ -247,6 +249,8 @@ struct gpusw_ctx {
   long long zip_iota_n = 0;
   int graphs = 1;              // replay cached plans as CUDA graphs
   int autotune = 1;            // tune stream shapes on first use
+  int stream_multi = 0;        // a batched call's streaming shapes in one launch (else one per shape)
+  int inter = 1;               // short explicit int16 pairs through the inter-sequence kernel where it pays
   std::vector<std::pair<std::pair<int, int>, std::vector<double>>> tune;  // (ns, P) -> us/row-pass
   gpusw_stats st{};
 };
@@ -690,6 +694,119 @@ void launch_pairs(gpusw_ctx* c, Bufs& B, int shape, int P, bool local, const gsw
   }
 }
 
+// Inter-sequence kernel (pairs_inter_kernel): one launch over all items, boundary columns
+// for every thread of the launch when a query is longer than one strip.
+template <bool L, bool T>
+void launch_inter_t(gpusw_ctx* c, Bufs& B, gsw::InterParams prm, int max_n, int max_m, const LaunchCfg& lc) {
+  auto k = gsw::pairs_inter_kernel<L, T>;
+  int bps = 1;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, 256, 0));
+  long long grid = (long long)c->sms * std::max(1, bps);
+  grid = std::max(1ll, std::min(grid, (prm.n_items + 255) / 256));
+  const bool strips = max_n > gsw::kInterW;
+  const size_t need = strips ? (size_t)grid * 256 * (size_t)std::max(1, max_m) : 0;
+  if (lc.need) {
+    *lc.need = need;
+    return;
+  }
+  prm.stride = grid * 256;
+  prm.bnd = strips ? (lc.bnd_off >= 0 ? static_cast<uint2*>(B.bnd.p) + lc.bnd_off : B.bnd.as<uint2>(need)) : nullptr;
+  k<<<(int)grid, 256, 0, lc.st ? lc.st : c->stream>>>(prm);
+  CK(cudaGetLastError());
+  c->st.last_launches++;
+}
+
+void launch_inter(gpusw_ctx* c, Bufs& B, const gsw::InterParams& prm, int max_n, int max_m,
+                  const LaunchCfg& lc = LaunchCfg()) {
+  const HostScheme& h = c->sch;
+  const bool local = h.mode == gsw::kModeLocal;
+  // the running maximum is needed in local mode, and elsewhere only as the int16 guard
+  const bool track = local || (long long)std::min(max_n, max_m) * std::max(0, h.max_sub) > prm.S.ovf_limit;
+  if (local) launch_inter_t<true, true>(c, B, prm, max_n, max_m, lc);
+  else if (track) launch_inter_t<false, true>(c, B, prm, max_n, max_m, lc);
+  else launch_inter_t<false, false>(c, B, prm, max_n, max_m, lc);
+}
+
+// Does the inter-sequence kernel apply to an int16 call over these query and reference sets?
+// Query codes 0..3 only (a 2-bit packed set) and every s - go of those columns in a byte.
+bool inter_applies(const gpusw_ctx* c, const Db& q, const Db& r, int P) {
+  const HostScheme& h = c->sch;
+  if (!c->inter || c->plain || P != 2 || q.bits != 2 || h.ns + 1 > gsw::kInterTabMax) return false;
+  auto words = [](const Db& d) {  // one past the set's last packed word
+    return d.n ? d.woff[d.n - 1] + (d.len[d.n - 1] + d.per - 1) / d.per + 1 : 0ll;
+  };
+  if (words(q) >= (1ll << 32) || words(r) >= (1ll << 32)) return false;  // 32-bit word offsets
+  for (int r = 0; r < h.ns; ++r)
+    for (int col = 0; col < 4 && col < h.ns; ++col) {
+      const int v = h.sub[(size_t)r * h.ns + col] - h.go;
+      if (v < -128 || v > 127) return false;
+    }
+  return true;
+}
+
+// Items of the inter-sequence kernel over the alignments `cand`: ordered by query length, then
+// reference length, longest first (two stable counting sorts), and neighbours paired into one
+// thread when their query lengths are equal (any neighbours in local mode); an unpaired
+// alignment takes a thread alone (b = -1). Also returns the largest item (query columns x the
+// longer reference) and the sum over items, which decide whether the kernel pays.
+struct InterPlan {
+  std::vector<int2> items;
+  int max_n = 0, max_m = 0;
+  double work = 0, max_work = 0;
+};
+
+InterPlan plan_inter(const Db& q, const Db& r, const int32_t* qi, const int32_t* rj,
+                     const std::vector<int>& cand, bool local) {
+  InterPlan pl;
+  const size_t n = cand.size();
+  for (int i : cand) {
+    pl.max_n = std::max(pl.max_n, q.len[qi[i]]);
+    pl.max_m = std::max(pl.max_m, r.len[rj[i]]);
+  }
+  const int max_n = pl.max_n, max_m = pl.max_m;
+  std::vector<int> by_m(n), order(n);
+  {
+    std::vector<int64_t> cnt((size_t)max_m + 2, 0);
+    for (int i : cand) cnt[(size_t)(max_m - r.len[rj[i]]) + 1]++;
+    for (int v = 0; v <= max_m; ++v) cnt[v + 1] += cnt[v];
+    for (int i : cand) by_m[cnt[(size_t)(max_m - r.len[rj[i]])]++] = i;
+  }
+  {
+    std::vector<int64_t> cnt((size_t)max_n + 2, 0);
+    for (int i : cand) cnt[(size_t)(max_n - q.len[qi[i]]) + 1]++;
+    for (int v = 0; v <= max_n; ++v) cnt[v + 1] += cnt[v];
+    for (size_t k = 0; k < n; ++k) {
+      const int i = by_m[k];
+      order[cnt[(size_t)(max_n - q.len[qi[i]])]++] = i;
+    }
+  }
+  pl.items.reserve((n + 1) / 2);
+  for (size_t k = 0; k < n;) {
+    const int a = order[k];
+    int b = -1;
+    if (k + 1 < n && (local || q.len[qi[order[k + 1]]] == q.len[qi[a]])) b = order[k + 1];
+    pl.items.push_back(make_int2(a, b));
+    k += b >= 0 ? 2 : 1;
+    const double w = (double)std::max(q.len[qi[a]], b >= 0 ? q.len[qi[b]] : 0) *
+                     std::max(r.len[rj[a]], b >= 0 ? r.len[rj[b]] : 0);
+    pl.work += w;
+    pl.max_work = std::max(pl.max_work, w);
+  }
+  return pl;
+}
+
+// Query length up to which an alignment goes to the inter-sequence kernel (four strips). On
+// uniform read/window-like pairs it measured 2.6x the team kernels at 30 x 40 residues, 1.2x at
+// 60 x 80 and 100 x 120, and 0.9x at 150 x 200, where the team kernel's 160-column pass fits.
+constexpr int kInterMaxCols = 128;
+
+// One thread scores a whole item, so the call takes as long as its longest item unless every
+// resident thread has several: the kernel is used when the items' work is at least twice the
+// largest item's on every resident thread (two 256-thread blocks per SM).
+bool inter_pays(const gpusw_ctx* c, const InterPlan& pl) {
+  return !pl.items.empty() && pl.work >= 2.0 * (double)c->sms * 512.0 * pl.max_work;
+}
+
 // Smallest pairs shape whose columns cover `ncols` and whose profile fits, else the widest
 // that fits (multi-pass).
 int pick_pair_shape(int ncols, int ns) {
@@ -877,6 +994,7 @@ const Db::Stream& get_stream(gpusw_ctx* c, Db& r, bool plain) {
   CK(cudaMemsetAsync(st.bytes, pad, std::max(1ll, cur), c->stream));
   CK(cudaMemcpyAsync(st.off, off.data(), off.size() * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(st.total, total.data(), total.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  st.total_h = total;
   if (r.n > 0) {
     long long* dst_d = nullptr;
     CK(cudaMalloc(&dst_d, r.n * sizeof(long long)));
@@ -952,6 +1070,41 @@ void launch_stream_shape(gpusw_ctx* c, Bufs& B, int shape, const gsw::StreamPara
     case 17: launch_stream_t<32, 28, P>(c, B, prm, mt, mp, lc); break;
     default: fail(GPUSW_ERR_INVALID, "bad stream kernel shape");
   }
+}
+
+// Every shape's items in one launch of cross_stream_multi_kernel (item.y = chunk | shape << 24).
+// smem: the largest profile among the call's shapes; boundary strips for 32 teams per CTA.
+template <int P>
+void launch_stream_multi(gpusw_ctx* c, Bufs& B, gsw::StreamParams prm, size_t smem, int n_streams_max_total,
+                         bool multipass, const LaunchCfg& lc) {
+  auto k = gsw::cross_stream_multi_kernel<P>;
+  static int configured_dev = -1;
+  static size_t configured_smem = 0;
+  if (configured_dev != c->device || configured_smem < smem) {
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(smem, configured_smem)));
+    configured_smem = std::max(smem, configured_smem);
+    configured_dev = c->device;
+  }
+  int bps = 1;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, 256, smem));
+  long long grid = (long long)c->sms * std::max(1, bps);
+  grid = std::max(1ll, std::min<long long>(grid, prm.n_items));
+  const long long strip = n_streams_max_total + 2 * gsw::kStreamPadLen;
+  const size_t need = multipass ? (size_t)grid * 32 * strip : 0;
+  if (lc.need) {
+    *lc.need = need;
+    return;
+  }
+  if (multipass) {
+    prm.bnd_strip = strip;
+    prm.bnd = lc.bnd_off >= 0 ? static_cast<uint2*>(B.bnd.p) + lc.bnd_off : B.bnd.as<uint2>(need);
+  } else {
+    prm.bnd = nullptr;
+    prm.bnd_strip = 0;
+  }
+  k<<<(int)grid, 256, smem, lc.st ? lc.st : c->stream>>>(prm);
+  CK(cudaGetLastError());
+  c->st.last_launches++;
 }
 
 // Cost of scoring `ncols` columns with a shape, per reference row (lane-steps x ops).
@@ -1139,9 +1292,43 @@ void run_cross_stream(gpusw_ctx* c, Bufs& B, const Db& q, Db& r, const int32_t* 
   Staging stg;
   const size_t off_pairs = stg.add(pairs.data(), pairs.size() * sizeof(int2));
   const size_t off_pout = stg.add(pair_out.data(), pair_out.size() * sizeof(int2));
-  struct L { int shape; size_t items_off; int n_items; bool multipass; };
+  struct L { int shape; size_t items_off; int n_items; bool multipass; size_t smem; };
   std::vector<L> launches;
+  int nshapes = 0, max_chunks = 0;
   for (int sh = 0; sh < kNumStream; ++sh) {
+    if (bins[sh].empty()) continue;
+    ++nshapes;
+    max_chunks = std::max(max_chunks, (st.n_streams + 256 / kStreamShapes[sh].G - 1) / (256 / kStreamShapes[sh].G));
+  }
+  // one launch for every shape (a batched, throughput-planned call of two or more shapes):
+  // items of all shapes in one queue, costliest first -- an item's time is its passes x the
+  // instructions of a step x the longest stream of its chunk (streams are sorted longest first)
+  const bool multi = c->stream_multi && !c->plain && !latency && nshapes >= 2 && max_chunks < (1 << 24);
+  if (multi) {
+    struct MI { double cost; int2 item; };
+    std::vector<MI> mi;
+    bool mp = false;
+    size_t smem = 0;
+    for (int sh = 0; sh < kNumStream; ++sh) {
+      if (bins[sh].empty()) continue;
+      const Shape S = kStreamShapes[sh];
+      const int nteams = 256 / S.G;
+      const int nchunks = (st.n_streams + nteams - 1) / nteams;
+      smem = std::max(smem, profile_bytes(S, h.ns));
+      for (int pi : bins[sh]) {
+        const int npass = (std::max(pair_cols[pi], 1) + S.cap() - 1) / S.cap();
+        mp |= npass > 1;
+        const double per = (double)npass * (5.5 * S.W + 6.0);
+        for (int ch = 0; ch < nchunks; ++ch)
+          mi.push_back({per * st.total_h[(size_t)ch * nteams], make_int2(pi, ch | sh << 24)});
+      }
+    }
+    std::stable_sort(mi.begin(), mi.end(), [](const MI& a, const MI& b) { return a.cost > b.cost; });
+    std::vector<int2> items(mi.size());
+    for (size_t i = 0; i < mi.size(); ++i) items[i] = mi[i].item;
+    launches.push_back({-1, stg.add(items.data(), items.size() * sizeof(int2)), (int)items.size(), mp, smem});
+  }
+  for (int sh = 0; sh < kNumStream && !multi; ++sh) {
     if (bins[sh].empty()) continue;
     const int nteams = 256 / kStreamShapes[sh].G;
     const int nchunks = (st.n_streams + nteams - 1) / nteams;
@@ -1151,7 +1338,7 @@ void run_cross_stream(gpusw_ctx* c, Bufs& B, const Db& q, Db& r, const int32_t* 
     items.reserve((size_t)nchunks * bins[sh].size());
     for (int ch = 0; ch < nchunks; ++ch)
       for (int pi : bins[sh]) items.push_back(make_int2(pi, ch));
-    launches.push_back({sh, stg.add(items.data(), items.size() * sizeof(int2)), (int)items.size(), mp});
+    launches.push_back({sh, stg.add(items.data(), items.size() * sizeof(int2)), (int)items.size(), mp, 0});
   }
   char* dmeta = stg.upload(c, B);
   const int nslots = (int)launches.size() + 2;
@@ -1182,8 +1369,14 @@ void run_cross_stream(gpusw_ctx* c, Bufs& B, const Db& q, Db& r, const int32_t* 
     lp.items = reinterpret_cast<const int2*>(dmeta + l.items_off);
     lp.n_items = l.n_items;
     lp.queue = reinterpret_cast<int*>(queues + i);
-    if (P == 2) launch_stream_shape<2>(c, B, l.shape, lp, st.max_total, l.multipass, lc);
-    else launch_stream_shape<1>(c, B, l.shape, lp, st.max_total, l.multipass, lc);
+    if (multi) {
+      if (P == 2) launch_stream_multi<2>(c, B, lp, l.smem, st.max_total, l.multipass, lc);
+      else launch_stream_multi<1>(c, B, lp, l.smem, st.max_total, l.multipass, lc);
+    } else if (P == 2) {
+      launch_stream_shape<2>(c, B, l.shape, lp, st.max_total, l.multipass, lc);
+    } else {
+      launch_stream_shape<1>(c, B, l.shape, lp, st.max_total, l.multipass, lc);
+    }
   });
   if (P == 2) launch_overflow_rescore(c, B, q, r, out, queues + launches.size());
 }
@@ -1456,6 +1649,7 @@ void begin_call(gpusw_ctx* c) {
   set_device(c);
   c->last_bufs = nullptr;
   c->st.last_launches = 0;
+  c->st.last_inter_items = 0;
   c->st.last_overflow = 0;
   c->st.last_pairs = 0;
   c->st.last_cells = 0;
@@ -2007,7 +2201,7 @@ int gpusw_score_cross(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qli
     const long long total = (long long)nq * r.n;
     const int P = choose_width(c, dtype, max_n, r.max_len);
     if (total > 0) ensure_tuned(c, P);
-    const std::vector<long long> key = {0, qdb, rdb, c->scheme_version, P, c->plain, nq, 0,
+    const std::vector<long long> key = {0, qdb, rdb, c->scheme_version, P, c->plain | c->stream_multi << 1 | c->inter << 2, nq, 0,
                                         (long long)fnv1a(qlist, (size_t)nq * 4)};
     auto body = [&](Bufs& B) {
       int* d_out = B.out.as<int>(total);
@@ -2087,7 +2281,7 @@ int gpusw_topk(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qlist, int
           }
         };
       };
-      const std::vector<long long> key = {1, qdb, rdb, c->scheme_version, P, c->plain, nq, kk,
+      const std::vector<long long> key = {1, qdb, rdb, c->scheme_version, P, c->plain | c->stream_multi << 1 | c->inter << 2, nq, kk,
                                           (long long)fnv1a(qlist, (size_t)nq * 4), c->mem_budget};
       CK(cudaEventRecord(c->ev1, c->stream));
       Bufs* B = &execute(c, key, !c->plain, body_w(P));
@@ -2164,13 +2358,26 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
     const HostScheme& h = c->sch;
     const bool local = h.mode == gsw::kModeLocal;
     int P = n > 0 ? choose_width(c, dtype, max_n, max_m) : 1;
-    const std::vector<long long> key = {2, qdb, rdb, c->scheme_version, P, c->plain, (long long)n, 0,
+    const std::vector<long long> key = {2, qdb, rdb, c->scheme_version, P, c->plain | c->stream_multi << 1 | c->inter << 2, (long long)n, 0,
                                         (long long)fnv1a(rj, (size_t)n * 4, fnv1a(qi, (size_t)n * 4))};
     Bufs* B = nullptr;
     tr.lap("validate+key");
     CK(cudaEventRecord(c->ev1, c->stream));
     // Plans the call on the host and runs it (recorded as a graph when cacheable).
     auto plan_and_run = [&](int Pw, bool cacheable) -> Bufs* {
+        // Short alignments (query <= kInterMaxCols) through the inter-sequence kernel when it
+        // applies and pays; they take the excluded shape kNumPair below.
+        InterPlan ipl;
+        bool use_inter = false;
+        if (inter_applies(c, q, r, Pw)) {
+          std::vector<int> cand;
+          for (int64_t i = 0; i < n; ++i)
+            if (q.len[qi[i]] <= kInterMaxCols) cand.push_back((int)i);
+          if (!cand.empty()) {
+            ipl = plan_inter(q, r, qi, rj, cand, local);
+            use_inter = inter_pays(c, ipl);
+          }
+        }
         // Plan (host, O(n), threaded): kernel shape per alignment from its column length, then
         // a stable order by (shape, row length descending) so int16x2 partners share a shape
         // and, mostly, a row length: the input order when it already is one (checked), else a
@@ -2184,8 +2391,8 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
         struct Part {
           long long lo = 0, hi = 0;
           bool sorted = true;
-          int mrow[kNumPair] = {}, mcol[kNumPair] = {};
-          long long cnt[kNumPair] = {};
+          int mrow[kNumPair + 1] = {}, mcol[kNumPair + 1] = {};
+          long long cnt[kNumPair + 1] = {};
         };
         std::vector<Part> part((size_t)host_threads() + 1);
         std::atomic<int> slot{0};
@@ -2199,7 +2406,9 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
           uint32_t prev = 0;
           for (long long i = lo; i < hi; ++i) {
             const int ql = q.len[qi[i]], rl = r.len[rj[i]];
-            const int sh = c->plain ? plain_shape : (ql <= 4096 ? shape_of_len[ql] : big);
+            const int sh = c->plain ? plain_shape
+                                    : (use_inter && ql <= kInterMaxCols) ? kNumPair
+                                    : (ql <= 4096 ? shape_of_len[ql] : big);
             shp[i] = (uint8_t)sh;
             pt.mrow[sh] = std::max(pt.mrow[sh], rl);
             pt.mcol[sh] = std::max(pt.mcol[sh], ql);
@@ -2213,15 +2422,15 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
         const int used = slot.load();
         std::sort(part.begin(), part.begin() + used, [](const Part& a, const Part& b) { return a.lo < b.lo; });
         bool sorted = true;
-        int mrow[kNumPair] = {}, mcol[kNumPair] = {};
-        long long cnt[kNumPair] = {};
+        int mrow[kNumPair + 1] = {}, mcol[kNumPair + 1] = {};
+        long long cnt[kNumPair + 1] = {};
         for (int t = 0; t < used; ++t) {
           const Part& pt = part[t];
           sorted &= pt.sorted;
           if (t > 0 && pt.hi > pt.lo && part[t - 1].hi > part[t - 1].lo &&
               key_of(pt.lo) < key_of(part[t - 1].hi - 1))
             sorted = false;
-          for (int sh = 0; sh < kNumPair; ++sh) {
+          for (int sh = 0; sh <= kNumPair; ++sh) {
             mrow[sh] = std::max(mrow[sh], pt.mrow[sh]);
             mcol[sh] = std::max(mcol[sh], pt.mcol[sh]);
             cnt[sh] += pt.cnt[sh];
@@ -2231,7 +2440,7 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
           std::iota(order.begin(), order.end(), 0);
         } else {
           const int mm = std::min(max_m, 0xFFFFFF);
-          const size_t nb = (size_t)kNumPair * ((size_t)mm + 1);
+          const size_t nb = (size_t)(kNumPair + 1) * ((size_t)mm + 1);
           if (nb <= (size_t)4 * n + 65536) {  // stable counting sort on (shape, mm - row length)
             auto bucket = [&](int64_t i) {
               return (size_t)shp[i] * ((size_t)mm + 1) + (size_t)(mm - std::min(r.len[rj[i]], 0xFFFFFF));
@@ -2258,21 +2467,24 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
         std::vector<Bin> plan_bins;
         {
           int64_t i0 = 0;
-          for (int sh = 0; sh < kNumPair; ++sh) {
+          for (int sh = 0; sh < kNumPair; ++sh) {  // shape kNumPair (inter-sequence) sorts last
             if (!cnt[sh]) continue;
             plan_bins.push_back({i0, i0 + cnt[sh], sh, mrow[sh], mcol[sh]});
             i0 += cnt[sh];
           }
         }
         tr.lap("plan");
-        Staging stg;  // qi, rj and order stay alive until the eager run has uploaded them
+        Staging stg;  // qi, rj, order and the inter items stay alive until the eager run has uploaded them
         const size_t o_qi = stg.add_ref(qi, (size_t)n * 4), o_rj = stg.add_ref(rj, (size_t)n * 4);
         const size_t o_ord = stg.add_ref(order.data(), (size_t)n * 4);
+        const size_t o_it = use_inter ? stg.add_ref(ipl.items.data(), ipl.items.size() * sizeof(int2)) : 0;
+        const int nb_team = (int)plan_bins.size();
         auto run = [&](int Pw) {
           return [&, Pw](Bufs& Bx) {
             char* dm = stg.upload(c, Bx);
             int* d_out = Bx.out.as<int>((size_t)n);
-            const int nslots = (int)plan_bins.size() + 2;
+            Bx.inter_items = use_inter ? (long long)ipl.items.size() : 0;
+            const int nslots = nb_team + 3;  // team bins, the overflow rescoring, the inter launch
             unsigned long long* queues = Bx.queue.as<unsigned long long>(nslots);
             staged(c, Bx, false, [&] {
               CK(cudaMemsetAsync(queues, 0, nslots * sizeof(unsigned long long), c->stream));
@@ -2289,7 +2501,27 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
               pp.ovf = Bx.ovf.as<gsw::Ovf>(kOvfCap);
               pp.ovf_count = Bx.ovf_count.as<int>(1);
               pp.ovf_cap = kOvfCap;
-              run_group(c, Bx, (int)plan_bins.size(), [&](int bi, const LaunchCfg& lc) {
+              gsw::InterParams ip{};
+              if (use_inter) {
+                ip.S = pp.S;
+                ip.sub = c->sub_d;
+                ip.cols = pp.cols;
+                ip.rows = pp.rows;
+                ip.qi = pp.qi;
+                ip.rj = pp.rj;
+                ip.items = reinterpret_cast<const int2*>(dm + o_it);
+                ip.n_items = (long long)ipl.items.size();
+                ip.queue = queues + nb_team + 1;
+                ip.out = d_out;
+                ip.ovf = pp.ovf;
+                ip.ovf_count = pp.ovf_count;
+                ip.ovf_cap = kOvfCap;
+              }
+              run_group(c, Bx, nb_team + (use_inter ? 1 : 0), [&](int bi, const LaunchCfg& lc) {
+                if (bi == nb_team) {
+                  launch_inter(c, Bx, ip, ipl.max_n, ipl.max_m, lc);
+                  return;
+                }
                 const Bin& bn = plan_bins[bi];
                 gsw::PairsParams lp = pp;
                 lp.order = reinterpret_cast<const int*>(dm + o_ord) + bn.i0;
@@ -2298,7 +2530,7 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
                 lp.queue = queues + bi;
                 launch_pairs(c, Bx, bn.shape, Pw, local, lp, bn.mrow, bn.mcol > kPairShapes[bn.shape].cap(), lc);
               });
-              if (Pw == 2) launch_overflow_rescore(c, Bx, q, r, d_out, queues + plan_bins.size());
+              if (Pw == 2) launch_overflow_rescore(c, Bx, q, r, d_out, queues + nb_team);
             });
           };
         };
@@ -2308,10 +2540,14 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
       Plan* hit = c->plain ? nullptr : lookup(c, key);
       B = hit ? &replay(c, hit) : plan_and_run(P, !c->plain);
       tr.lap(hit ? "replay" : "run");
+      c->st.last_inter_items = B->inter_items;
       if (P == 2) {
         const int n_ovf = read_overflow_count(c, *B);
         c->st.last_overflow = n_ovf;
-        if (n_ovf > kOvfCap) B = plan_and_run(1, false);  // too many flagged cells: all int32
+        if (n_ovf > kOvfCap) {  // too many flagged cells: all int32
+          B = plan_and_run(1, false);
+          c->st.last_inter_items = 0;
+        }
       }
     }
     c->last_bufs = B;
@@ -2860,6 +3096,8 @@ int gpusw_set_options(gpusw_ctx* c, int plain, int64_t mem_budget, int flags) {
     c->mem_budget = mem_budget ? mem_budget : (4ll << 30);
     c->autotune = (flags & GPUSW_OPT_NO_AUTOTUNE) ? 0 : 1;
     c->graphs = (flags & GPUSW_OPT_NO_GRAPHS) ? 0 : 1;
+    c->stream_multi = (flags & GPUSW_OPT_ONE_LAUNCH) ? 1 : 0;
+    c->inter = (flags & GPUSW_OPT_NO_INTER) ? 0 : 1;
   });
 }
 

@@ -552,80 +552,123 @@ struct StreamParams {
   long long bnd_strip;        // entries per strip (max stream total + 2 pads)
 };
 
+// One work item of the streaming kernel: (column pair, chunk of nteams streams), every column
+// pass of the pair scored by the CTA's teams, one stream each, and the stream's scores written.
+// bnd_teams: boundary strips reserved per CTA (the CTA's teams, or the most any shape has).
 template <int G, int W, int P>
-__global__ void __launch_bounds__(256) cross_stream_kernel(const StreamParams p) {
-  extern __shared__ uint4 smem_prof[];
-  __shared__ int s_item;
-  __shared__ uint32_t s_part[256 * kStreamRows];
+__device__ __forceinline__ void stream_item(const StreamParams& p, const int2 item, uint4* smem_prof,
+                                            uint32_t* s_part, int bnd_teams) {
   constexpr int SLOTS = G * W / 4;
   const int pstride = (SLOTS + 7) & ~7;
   const int team = threadIdx.x / G, lane = threadIdx.x % G, nteams = blockDim.x / G;
   const unsigned wmask = (G == 32) ? 0xFFFFFFFFu
                                    : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
   uint32_t* part = s_part + team * kStreamRows * G;
-  uint2* bnd = p.bnd ? p.bnd + ((long long)blockIdx.x * nteams + team) * p.bnd_strip + kStreamPadLen
+  uint2* bnd = p.bnd ? p.bnd + ((long long)blockIdx.x * bnd_teams + team) * p.bnd_strip + kStreamPadLen
                      : nullptr;
   const uint32_t GO = V<P>::splat(p.S.go);
+  const int2 pr = p.pairs[item.x], po = p.pair_out[item.x];
+  const int n0 = pr.x >= 0 ? p.cols.len[pr.x] : 0;
+  const int n1 = (P == 2 && pr.y >= 0) ? p.cols.len[pr.y] : 0;
+  const int ncols = max(max(n0, n1), 1);
+  const int npass = (ncols + G * W - 1) / (G * W);
+  const int s = item.y * nteams + team;
+  const bool have = s < p.n_streams;
+  const int total = have ? p.stream_total[s] : 0;
+#pragma unroll
+  for (int q = 0; q < kStreamRows; ++q) part[q * G + lane] = GO;
+  for (int ps = 0; ps < npass; ++ps) {
+    __syncthreads();
+    build_profile<G, W, P>(p.S, p.sub, p.cols, pr.x, n0, P == 2 ? pr.y : -1, n1, ps * G * W,
+                           smem_prof, pstride, threadIdx.x, blockDim.x);
+    __syncthreads();
+    if (total > 0)
+      team_stream_local<G, W, P>(p.S, smem_prof, pstride, p.stream + p.stream_off[s], total, bnd,
+                                 ps > 0, ps + 1 < npass, lane, wmask, part);
+  }
+  __syncwarp(wmask);
+  // lane j < kStreamRows writes the scores of the stream's j-th reference
+  if (have && lane < kStreamRows) {
+    const int pos = s * kStreamRows + lane;
+    if (pos < p.n_rows) {
+      const int rs = p.row_perm[pos];
+      const int m = p.row_len[rs];
+      int slot = 0;
+      for (int j = 0; j < lane; ++j)
+        if (p.row_len[p.row_perm[s * kStreamRows + j]] > 0) ++slot;
+      uint32_t best = GO;
+      if (m > 0)
+        for (int l = 0; l < G; ++l) best = V<P>::max2(best, part[slot * G + l]);
+#pragma unroll
+      for (int h = 0; h < P; ++h) {
+        const int c = h ? pr.y : pr.x;
+        if (c < 0) continue;
+        const int nh = h ? n1 : n0;
+        const long long opos = (long long)(h ? po.y : po.x) * p.out_ld + rs;
+        int score;
+        if (m == 0 || nh == 0) {
+          score = 0;  // local mode: an empty side scores 0
+        } else {
+          score = V<P>::get(best, h) - p.S.go;
+          if (P == 2 && score > p.S.ovf_limit) {
+            push_overflow(p.ovf, p.ovf_count, p.ovf_cap, c, rs, opos);
+            score = INT_MIN;
+          }
+        }
+        p.out[opos] = score;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// One shape per launch: persistent CTAs take items (pair, chunk) from the launch's queue.
+template <int G, int W, int P>
+__global__ void __launch_bounds__(256) cross_stream_kernel(const StreamParams p) {
+  extern __shared__ uint4 smem_prof[];
+  __shared__ int s_item;
+  __shared__ uint32_t s_part[256 * kStreamRows];
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(p.queue, 1);
     __syncthreads();
     const int it = s_item;
     __syncthreads();
     if (it >= p.n_items) break;
-    const int2 item = p.items[it];
-    const int2 pr = p.pairs[item.x], po = p.pair_out[item.x];
-    const int n0 = pr.x >= 0 ? p.cols.len[pr.x] : 0;
-    const int n1 = (P == 2 && pr.y >= 0) ? p.cols.len[pr.y] : 0;
-    const int ncols = max(max(n0, n1), 1);
-    const int npass = (ncols + G * W - 1) / (G * W);
-    const int s = item.y * nteams + team;
-    const bool have = s < p.n_streams;
-    const int total = have ? p.stream_total[s] : 0;
-#pragma unroll
-    for (int q = 0; q < kStreamRows; ++q) part[q * G + lane] = GO;
-    for (int ps = 0; ps < npass; ++ps) {
-      __syncthreads();
-      build_profile<G, W, P>(p.S, p.sub, p.cols, pr.x, n0, P == 2 ? pr.y : -1, n1, ps * G * W,
-                             smem_prof, pstride, threadIdx.x, blockDim.x);
-      __syncthreads();
-      if (total > 0)
-        team_stream_local<G, W, P>(p.S, smem_prof, pstride, p.stream + p.stream_off[s], total, bnd,
-                                   ps > 0, ps + 1 < npass, lane, wmask, part);
-    }
-    __syncwarp(wmask);
-    // lane j < kStreamRows writes the scores of the stream's j-th reference
-    if (have && lane < kStreamRows) {
-      const int pos = s * kStreamRows + lane;
-      if (pos < p.n_rows) {
-        const int rs = p.row_perm[pos];
-        const int m = p.row_len[rs];
-        int slot = 0;
-        for (int j = 0; j < lane; ++j)
-          if (p.row_len[p.row_perm[s * kStreamRows + j]] > 0) ++slot;
-        uint32_t best = GO;
-        if (m > 0)
-          for (int l = 0; l < G; ++l) best = V<P>::max2(best, part[slot * G + l]);
-#pragma unroll
-        for (int h = 0; h < P; ++h) {
-          const int c = h ? pr.y : pr.x;
-          if (c < 0) continue;
-          const int nh = h ? n1 : n0;
-          const long long opos = (long long)(h ? po.y : po.x) * p.out_ld + rs;
-          int score;
-          if (m == 0 || nh == 0) {
-            score = 0;  // local mode: an empty side scores 0
-          } else {
-            score = V<P>::get(best, h) - p.S.go;
-            if (P == 2 && score > p.S.ovf_limit) {
-              push_overflow(p.ovf, p.ovf_count, p.ovf_cap, c, rs, opos);
-              score = INT_MIN;
-            }
-          }
-          p.out[opos] = score;
-        }
-      }
-    }
+    stream_item<G, W, P>(p, p.items[it], smem_prof, s_part, 256 / G);
+  }
+}
+
+// The streaming kernel's shapes, by index: (index, G, W). The host's shape table and its
+// per-shape launches are generated from the same list.
+#define GSW_STREAM_SHAPES(X)                                                              \
+  X(0, 8, 4) X(1, 8, 8) X(2, 8, 12) X(3, 8, 16) X(4, 8, 24) X(5, 8, 32) X(6, 16, 16)     \
+  X(7, 16, 20) X(8, 16, 24) X(9, 16, 32) X(10, 32, 16) X(11, 32, 20) X(12, 32, 24)         \
+  X(13, 32, 32) X(14, 8, 20) X(15, 8, 28) X(16, 16, 28) X(17, 32, 28)
+
+// Every shape in one launch (a length-scheduled call): one queue of items across shapes,
+// ordered by the host longest first; item.y = chunk | shape << 24. Each CTA switches its team
+// layout to the item's shape; the dynamic shared memory holds the largest profile of the call,
+// and boundary strips are reserved for 32 teams per CTA (the most any shape has).
+template <int P>
+__global__ void __launch_bounds__(256) cross_stream_multi_kernel(const StreamParams p) {
+  extern __shared__ uint4 smem_prof[];
+  __shared__ int s_item;
+  __shared__ uint32_t s_part[256 * kStreamRows];
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(p.queue, 1);
     __syncthreads();
+    const int it = s_item;
+    __syncthreads();
+    if (it >= p.n_items) break;
+    const int2 raw = p.items[it];
+    const int2 item = make_int2(raw.x, raw.y & 0xFFFFFF);
+    switch ((unsigned)raw.y >> 24) {
+#define GSW_MULTI_CASE(IDX, G_, W_) \
+  case IDX: stream_item<G_, W_, P>(p, item, smem_prof, s_part, 32); break;
+      GSW_STREAM_SHAPES(GSW_MULTI_CASE)
+#undef GSW_MULTI_CASE
+      default: break;
+    }
   }
 }
 
@@ -742,6 +785,269 @@ __global__ void __launch_bounds__(256) pairs_noalloc_kernel(const NoAllocParams 
       else if (LEFTPAD) score = finish_score_leftpad<1>(p.S, acc, 0, &ovf);
       else score = finish_score<1>(p.S, acc, 0, &ovf);
       p.out[k] = score;
+    }
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// Inter-sequence pairs kernel: one thread scores two alignments from start to end, as the
+// low and high int16 halves of every register -- no team, no shuffles, no wavefront skew.
+//
+// Columns (query) are scored in strips of up to W held in registers: per column its H + go
+// (HGO), its F and a byte-permute selector. The substitution value of a cell is one `prmt`:
+// the row's table word of each half (four int8 values s - go, one per column code 0..3, from
+// a shared table of ns + 1 words: entry ns is the pad row, 0) indexed by the column's
+// selector, whose nibbles pick byte q of the low half's word and byte 4 + q of the high
+// half's, each followed by its sign byte. A cell then costs the byte permute, three DPX ops
+// (E and F add-max, H max3) and two vadd2 (H + s and H + go). Past a query's end the
+// selector nibbles are 8 (the sign of byte 0: s' = 0 or -1, so s <= go <= 0); past a
+// reference's end the row uses the pad entry (s' = 0).
+//
+// A strip boundary -- (HGO, E) of the strip's last column for every row -- goes through a
+// per-thread column of `bnd`, entry (row * stride), overwritten in place by the next strip.
+//
+// Applies when the query set holds only codes 0..3 (2-bit packed) and every s - go of those
+// columns fits a signed byte. Both alignments of a thread have the same query length unless
+// the scheme is local (ends past a query only lower a local score); references may differ.
+// Results follow the reference's recurrence (src/gpusw/reference.py:58-125) exactly as the
+// team kernels do: HGO units, captures of the corner, the last column (free query end) and
+// the last row (free reference end) per half.
+struct InterParams {
+  SchemeDev S;
+  const int* sub;
+  Packed cols, rows;
+  const int* qi;
+  const int* rj;
+  const int2* items;          // (alignment a, alignment b or -1), longest first
+  long long n_items;
+  unsigned long long* queue;  // items taken 32 at a time per warp, zero at launch
+  uint2* bnd;                 // boundary columns, bnd[row * stride + thread]
+  long long stride;           // threads of the launch
+  int* out;
+  Ovf* ovf;
+  int* ovf_count;
+  int ovf_cap;
+};
+
+constexpr int kInterW = 32;       // columns per strip
+constexpr int kInterTabMax = 65;  // row table words (ns + 1 <= 65)
+
+struct InterItem {
+  int n, na, nb, ma, mb, M;
+  uint32_t qa, qb;  // first packed word of each query (the host keeps word counts below 2^32)
+  uint32_t ra, rb;  // first packed word of each reference
+  Acc acc;
+};
+
+__device__ __forceinline__ uint32_t prmt_sel(uint32_t lo, uint32_t hi, uint32_t sel) {
+  uint32_t d;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(lo), "r"(hi), "r"(sel));
+  return d;
+}
+
+// One strip of WL4 columns starting at column s0 (0-based; s0 % 16 == 0). dd = WL4 - (real
+// columns of the last strip), 0..3, so the query's last column is register WL4 - 1 - dd.
+template <int WL4, bool FIRST, bool LAST, bool LOCAL, bool TRACK>
+__device__ __forceinline__ void inter_strip(const InterParams& p, const uint32_t* s_tab, uint4* s_q,
+                                            InterItem& it, int s0, int dd, uint2* bnd) {
+  const SchemeDev& S = p.S;
+  const uint32_t GO = V<2>::splat(S.go), GE = V<2>::splat(S.ge), NEGF = V<2>::splat(S.neg_f);
+  // column selectors from the 2-bit codes of both queries (two words cover 32 columns), kept
+  // in the thread's shared-memory column s_q[g * blockDim.x] (four per uint4) to leave the
+  // registers to the strip's HGO and F
+  {
+    uint32_t Q[WL4];
+    const int w0 = s0 >> 4;
+    const uint32_t* qw = p.cols.words;
+    const uint32_t a0 = it.na > s0 ? __ldg(qw + it.qa + w0) : 0u;
+    const uint32_t a1 = (WL4 > 16 && it.na > s0 + 16) ? __ldg(qw + it.qa + w0 + 1) : 0u;
+    const uint32_t b0 = it.nb > s0 ? __ldg(qw + it.qb + w0) : 0u;
+    const uint32_t b1 = (WL4 > 16 && it.nb > s0 + 16) ? __ldg(qw + it.qb + w0 + 1) : 0u;
+#pragma unroll
+    for (int k = 0; k < WL4; ++k) {
+      const uint32_t ca = ((k < 16 ? a0 >> (2 * k) : a1 >> (2 * (k - 16))) & 3u);
+      const uint32_t cb = ((k < 16 ? b0 >> (2 * k) : b1 >> (2 * (k - 16))) & 3u);
+      const uint32_t qa = s0 + k < it.na ? ca * 0x11u + 0x80u : 0x88u;
+      const uint32_t qb = s0 + k < it.nb ? (cb * 0x11u + 0xC4u) << 8 : 0x8800u;
+      Q[k] = qa | qb;
+    }
+#pragma unroll
+    for (int g = 0; g < WL4 / 4; ++g)
+      s_q[g * blockDim.x] = make_uint4(Q[4 * g], Q[4 * g + 1], Q[4 * g + 2], Q[4 * g + 3]);
+  }
+  // row 0: the top boundary H(0, j), F = -inf
+  uint32_t Hgo[WL4], F[WL4];
+#pragma unroll
+  for (int k = 0; k < WL4; ++k) {
+    Hgo[k] = V<2>::splat(edge_value(S, S.free_r, s0 + k + 1) + S.go);
+    F[k] = NEGF;
+  }
+  uint32_t dleft = V<2>::splat(edge_value(S, S.free_r, s0) + S.go);  // HGO(i - 1, s0)
+  // left boundary of the first strip: H(i, 0) = 0 or the gap ladder, E = -inf
+  const bool ladder = !(S.mode == kModeLocal || (S.mode == kModeSemi && S.free_q));
+  uint32_t lad = V<2>::splat(ladder ? 2 * S.go : S.go);  // HGO(1, 0)
+  // row codes: one packed word per `per` rows for each half; the table words of the next row
+  // are fetched while the current row is scored
+  const int rbits = p.rows.bits, rper = p.rows.per;
+  const uint32_t rmask = (1u << rbits) - 1u;
+  const uint32_t* rw = p.rows.words;
+  uint32_t wa = it.ma > 0 ? __ldg(rw + it.ra) : 0u, wb = it.mb > 0 ? __ldg(rw + it.rb) : 0u;
+  int rpos = 0;
+  uint32_t rwa = it.ra, rwb = it.rb;  // word offsets of the current row words
+  auto row_tab = [&](int i, uint32_t& ta, uint32_t& tb) {  // table words of row i, then advance
+    ta = s_tab[i < it.ma ? (int)(wa & rmask) : S.ns];
+    tb = s_tab[i < it.mb ? (int)(wb & rmask) : S.ns];
+    wa >>= rbits;
+    wb >>= rbits;
+    if (++rpos == rper) {
+      rpos = 0;
+      ++rwa;
+      ++rwb;
+      wa = i + 1 < it.ma ? __ldg(rw + rwa) : 0u;
+      wb = i + 1 < it.mb ? __ldg(rw + rwb) : 0u;
+    }
+  };
+  uint32_t TA = 0, TB = 0;
+  if (it.M > 0) row_tab(0, TA, TB);
+  uint2* bp = bnd;  // this row's boundary entry
+  uint2 nb = make_uint2(0u, 0u);
+  if (!FIRST) nb = *bp;
+  const uint32_t v_neg = V<2>::splat(S.neg_low);
+  for (int i = 0; i < it.M; ++i) {
+    const uint32_t ta = TA, tb = TB;
+    if (i + 1 < it.M) row_tab(i + 1, TA, TB);
+    uint32_t hl, e;
+    if (FIRST) {
+      hl = lad;
+      e = NEGF;
+      if (ladder) lad = __vadd2(lad, GE);
+    } else {
+      hl = nb.x;
+      e = nb.y;
+      if (i + 1 < it.M) nb = bp[p.stride];
+    }
+    uint32_t d = dleft, hgo_l = hl;
+    dleft = hl;
+#pragma unroll
+    for (int k = 0; k < WL4; ++k) {
+      const uint4 q4 = s_q[(k >> 2) * blockDim.x];
+      const uint32_t qk = (k & 3) == 0 ? q4.x : (k & 3) == 1 ? q4.y : (k & 3) == 2 ? q4.z : q4.w;
+      const uint32_t ds = __vadd2(d, prmt_sel(ta, tb, qk));
+      e = __viaddmax_s16x2(e, GE, hgo_l);
+      const uint32_t f = __viaddmax_s16x2(F[k], GE, Hgo[k]);
+      const uint32_t h = LOCAL ? __vimax3_s16x2_relu(ds, e, f) : __vimax3_s16x2(ds, e, f);
+      d = Hgo[k];
+      F[k] = f;
+      Hgo[k] = __vadd2(h, GO);
+      hgo_l = Hgo[k];
+      if (TRACK && (k & 1)) it.acc.best = __vimax3_s16x2(it.acc.best, Hgo[k - 1], Hgo[k]);
+    }
+    if (!LAST) *bp = make_uint2(Hgo[WL4 - 1], e);
+    bp += p.stride;
+    if (!LOCAL) {
+      if (LAST && S.mode == kModeSemi && S.free_q) {  // H(i, n) of the rows each half has
+        const uint32_t v = dd == 0 ? Hgo[WL4 - 1] : dd == 1 ? Hgo[WL4 - 2] : dd == 2 ? Hgo[WL4 - 3] : Hgo[WL4 - 4];
+        const uint32_t live = (i < it.ma ? 0x0000FFFFu : 0u) | (i < it.mb ? 0xFFFF0000u : 0u);
+        it.acc.endcol = __vmaxs2(it.acc.endcol, (v & live) | (v_neg & ~live));
+      }
+      if (i == it.ma - 1 || i == it.mb - 1) {  // a half's last row: corner and last-row maximum
+        const uint32_t half = (i == it.ma - 1 ? 0x0000FFFFu : 0u) | (i == it.mb - 1 ? 0xFFFF0000u : 0u);
+        uint32_t rmax = v_neg;
+#pragma unroll
+        for (int k = 0; k < WL4; ++k)
+          if (!LAST || k < WL4 - 4 || k < WL4 - dd) rmax = __vmaxs2(rmax, Hgo[k]);
+        it.acc.endrow = __vmaxs2(it.acc.endrow, (rmax & half) | (v_neg & ~half));
+        if (LAST) {
+          const uint32_t v = dd == 0 ? Hgo[WL4 - 1] : dd == 1 ? Hgo[WL4 - 2] : dd == 2 ? Hgo[WL4 - 3] : Hgo[WL4 - 4];
+          it.acc.corner = (v & half) | (it.acc.corner & ~half);
+        }
+      }
+    }
+  }
+}
+
+template <bool FIRST, bool LOCAL, bool TRACK>
+__device__ __forceinline__ void inter_last_strip(const InterParams& p, const uint32_t* s_tab, uint4* s_q,
+                                                 InterItem& it, int s0, uint2* bnd) {
+  const int wl = it.n - s0, wl4 = (wl + 3) & ~3, dd = wl4 - wl;
+  switch (wl4 >> 2) {
+    case 1: inter_strip<4, FIRST, true, LOCAL, TRACK>(p, s_tab, s_q, it, s0, dd, bnd); break;
+    case 2: inter_strip<8, FIRST, true, LOCAL, TRACK>(p, s_tab, s_q, it, s0, dd, bnd); break;
+    case 3: inter_strip<12, FIRST, true, LOCAL, TRACK>(p, s_tab, s_q, it, s0, dd, bnd); break;
+    case 4: inter_strip<16, FIRST, true, LOCAL, TRACK>(p, s_tab, s_q, it, s0, dd, bnd); break;
+    case 5: inter_strip<20, FIRST, true, LOCAL, TRACK>(p, s_tab, s_q, it, s0, dd, bnd); break;
+    case 6: inter_strip<24, FIRST, true, LOCAL, TRACK>(p, s_tab, s_q, it, s0, dd, bnd); break;
+    case 7: inter_strip<28, FIRST, true, LOCAL, TRACK>(p, s_tab, s_q, it, s0, dd, bnd); break;
+    default: inter_strip<32, FIRST, true, LOCAL, TRACK>(p, s_tab, s_q, it, s0, dd, bnd); break;
+  }
+}
+
+// Persistent: each warp takes 32 consecutive items per queue step (one per lane); the host
+// orders items by query length then reference length, longest first, so a warp's lanes run
+// strips of the same widths over similar row counts.
+template <bool LOCAL, bool TRACK>
+__global__ void __launch_bounds__(256, 2) pairs_inter_kernel(const InterParams p) {
+  static_assert(kInterW == 32, "two packed query words per strip");
+  __shared__ uint32_t s_tab[kInterTabMax];
+  __shared__ uint4 s_qsel[kInterW / 4 * 256];
+  uint4* s_q = s_qsel + threadIdx.x;
+  const SchemeDev& S = p.S;
+  for (int r = threadIdx.x; r <= S.ns; r += blockDim.x) {
+    uint32_t w = 0;
+    if (r < S.ns)
+      for (int c = 0; c < 4 && c < S.ns; ++c) w |= (uint32_t)((p.sub[r * S.ns + c] - S.go) & 0xFF) << (8 * c);
+    s_tab[r] = w;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  uint2* bnd = p.bnd ? p.bnd + (long long)blockIdx.x * blockDim.x + threadIdx.x : nullptr;
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(p.queue, 32ull);
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if ((long long)base >= p.n_items) break;
+    const long long t = (long long)base + lane;
+    if (t >= p.n_items) continue;
+    const int2 ab = p.items[t];
+    const int a = ab.x, b = ab.y >= 0 ? ab.y : ab.x;
+    InterItem it;
+    const int qa = p.qi[a], ra = p.rj[a], qb = p.qi[b], rb = p.rj[b];
+    it.na = p.cols.len[qa];
+    it.nb = p.cols.len[qb];
+    it.ma = p.rows.len[ra];
+    it.mb = p.rows.len[rb];
+    it.n = max(it.na, it.nb);
+    it.M = max(it.ma, it.mb);
+    it.qa = (uint32_t)p.cols.woff[qa];
+    it.qb = (uint32_t)p.cols.woff[qb];
+    it.ra = (uint32_t)p.rows.woff[ra];
+    it.rb = (uint32_t)p.rows.woff[rb];
+    it.acc = init_acc<2>(S);
+    if (it.n > 0 && it.M > 0) {
+      const int nstrip = (it.n + kInterW - 1) / kInterW;
+      if (nstrip == 1) {
+        inter_last_strip<true, LOCAL, TRACK>(p, s_tab, s_q, it, 0, bnd);
+      } else {
+        inter_strip<kInterW, true, false, LOCAL, TRACK>(p, s_tab, s_q, it, 0, 0, bnd);
+        for (int sx = 1; sx + 1 < nstrip; ++sx)
+          inter_strip<kInterW, false, false, LOCAL, TRACK>(p, s_tab, s_q, it, sx * kInterW, 0, bnd);
+        inter_last_strip<false, LOCAL, TRACK>(p, s_tab, s_q, it, (nstrip - 1) * kInterW, bnd);
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (h == 1 && ab.y < 0) continue;
+      const int nh = h ? it.nb : it.na, mh = h ? it.mb : it.ma;
+      bool ovf = false;
+      int score;
+      if (nh == 0 || mh == 0) score = empty_score(S, nh, mh);
+      else score = finish_score<2>(S, it.acc, h, &ovf);
+      const int al = h ? ab.y : a;
+      if (ovf && nh > 0 && mh > 0) {
+        push_overflow(p.ovf, p.ovf_count, p.ovf_cap, h ? qb : qa, h ? rb : ra, al);
+        score = INT_MIN;
+      }
+      p.out[al] = score;
     }
   }
 }

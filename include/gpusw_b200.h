@@ -66,6 +66,8 @@ typedef struct gpusw_stats {
   int64_t total_launches;     /* kernels launched by this context */
   int64_t total_overflow;     /* int16 rescores over the context's lifetime */
   int64_t device_bytes;       /* device memory currently held by the context */
+  int64_t last_inter_items;   /* threads' items (one or two alignments) of the last call that
+                                 the inter-sequence pairs kernel scored */
 } gpusw_stats;
 
 /* Library version (major * 10000 + minor * 100 + patch). */
@@ -178,9 +180,19 @@ int gpusw_locate_pairs(gpusw_ctx *ctx, int32_t qdb, int32_t rdb, const int32_t *
  * one kernel shape per batch, no length binning, no graph) used as the comparison point
  * of the batched form. mem_budget bounds the score blocks of gpusw_topk (bytes, 0 keeps the
  * default of 4 GiB). flags: GPUSW_OPT_NO_AUTOTUNE keeps the modelled kernel-shape costs,
- * GPUSW_OPT_NO_GRAPHS runs every call eagerly instead of replaying cached CUDA graphs. */
+ * GPUSW_OPT_NO_GRAPHS runs every call eagerly instead of replaying cached CUDA graphs,
+ * GPUSW_OPT_ONE_LAUNCH scores a local-mode cross product of several streaming-kernel shapes
+ * in one persistent launch over every shape's work items (costliest first) instead of one
+ * launch per shape on up to four streams (the default: on the uneven-length protein top-10
+ * the single launch measured 7 % slower, its registers being the most any shape needs),
+ * GPUSW_OPT_NO_INTER keeps every explicit pair on the team kernels (by default, int16 pairs
+ * of queries up to 128 residues go to the inter-sequence kernel, one thread per two
+ * alignments, when the query set holds only codes 0..3, the scheme's values fit a byte and
+ * the call has enough of them to keep every thread busy). */
 #define GPUSW_OPT_NO_AUTOTUNE 1
 #define GPUSW_OPT_NO_GRAPHS 2
+#define GPUSW_OPT_ONE_LAUNCH 4
+#define GPUSW_OPT_NO_INTER 8
 int gpusw_set_options(gpusw_ctx *ctx, int plain, int64_t mem_budget, int flags);
 
 /* Autotune the streaming cross-product kernel for the current scheme: every compiled

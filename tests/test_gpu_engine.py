@@ -175,3 +175,39 @@ def test_global_cross_multi_shape_bins():
         want = oracle.score_cross(funnel(qs, sch), funnel(rs, sch), sch)
         for _ in range(3):
             assert np.array_equal(al.score_cross().astype(np.int64), want)
+
+
+@pytest.mark.parametrize("sch", [schemes.DNA, schemes.BLOSUM62.replace(dtype="int32"),
+                                 Scheme(mode="local", match=900, mismatch=-3, gap_open=-5, gap_extend=-2)],
+                         ids=["dna-int16", "blosum62-int32", "int16-overflow"])
+def test_one_launch_option_equals_oracle(sch):
+    """GPUSW_OPT_ONE_LAUNCH: every streaming shape of a call (single- and multi-pass, query
+    lengths 5..2,500) in one persistent launch. Scores and top-k equal the default launches;
+    a 3,000-cell sample of the matrix equals the oracle."""
+    alpha = "ACGT" if sch.eff_alphabet == "ACGT" else "ARNDCQEGHILKMFPSTWYV"
+    rng = np.random.default_rng(61)
+    qs = rand_seqs(rng, 200, 5, 2500, alpha)
+    rs = rand_seqs(rng, 1000, 5, 400, alpha)
+    if sch.match == 900:
+        rs[:40] = [q[:300] for q in qs[:40]]  # identical stretches: int16 overflow, rescored
+    ctx = _native.context(0)
+    al = Aligner(sch).index(rs).set_queries(qs)
+    default = al.score_cross()
+    dtk = al.top_k(k=9)
+    try:
+        ctx.set_options(one_launch=True)
+        for _ in range(3):  # eager, recorded, replayed
+            assert np.array_equal(al.score_cross(), default)
+        tk = al.top_k(k=9)
+        assert ctx.stats().last_launches >= 1
+    finally:
+        ctx.set_options()
+    assert np.array_equal(tk.topk_idx, dtk.topk_idx) and np.array_equal(tk.topk_scores, dtk.topk_scores)
+    qi = rng.integers(0, 200, 3000).astype(np.int32)
+    rj = rng.integers(0, 1000, 3000).astype(np.int32)
+    qi[:40] = np.arange(40)
+    rj[:40] = np.arange(40)
+    want = oracle.score_pairs(funnel(qs, sch), funnel(rs, sch), qi, rj, sch)
+    assert np.array_equal(default[qi, rj].astype(np.int64), want)
+    if sch.match == 900:
+        assert default.max() > 32767

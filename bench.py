@@ -396,20 +396,21 @@ def hbm_peak():
         return 6650.0, "fallback 6.65 TB/s (earlier measurement on this pool)"
 
 
-def roofline(cells, score_ms, dpx, wl=None, bits=None):
+def roofline(cells, score_ms, dpx, wl=None):
     """Scoring kernels against the per-pipe instruction ceilings (GCUPS)."""
     alu = dpx * 2.0 / ALU_OPS_PER_REG / 1e9
     fma = dpx * 2.0 / FMA_OPS_PER_REG / 1e9
     achieved = cells / (score_ms * 1e-3) / 1e9 if score_ms > 0 else 0.0
-    traffic, src = None, ("not extrapolated: the references (packed words and stream bytes) "
-                          "are L2-resident and reused by every query pair")
-    if wl is not None and wl.pairs is not None and bits is not None:
-        # the pairs kernel reads each pair's packed words once plus 12 B of per-sequence
-        # metadata, 8 B of pair indices and 4 B of output (the ncu capture of 100,000 such
-        # pairs read 14.9 MB, 1.6 x the packed words, from this metadata and 32-byte sectors)
-        n = wl.pairs[0].shape[0]
-        traffic = float(packed_bytes(wl.queries[1], bits) + packed_bytes(wl.refs[1], bits) + 12 * n)
-        src = "algorithmic bytes of the launch (packed words + metadata + indices + output)"
+    traffic, src = None, ("not extrapolated: no DRAM capture of this kernel at this workload's "
+                          "lengths and alphabet")
+    if wl is not None and wl.name == "pairs" and wl.pairs is not None:
+        # measured: dram__bytes_read.sum + dram__bytes_write.sum of the pairs kernel on 100,000
+        # of these 150/200-residue pairs = 14,885,120 + 0 B (the scores stay in L2 until the
+        # launch ends): 148.85 B per pair, the packed words of both sides read once plus the
+        # per-sequence metadata in 32-byte sectors; traffic grows with the pair count
+        traffic = 148.8512 * wl.pairs[0].shape[0]
+        src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of pairs_kernel<8,20,2> on "
+               "100,000 pairs of this workload (14,885,120 B), scaled by the pair count")
     return {"bound": "int", "achieved": achieved, "peak": alu, "unit": "GCUPS",
             "frac": achieved / alu if alu else None, "peak_pipe": "alu",
             "ceilings_gcups": {"alu": alu, "fma": fma},
@@ -528,7 +529,7 @@ def measure(ctx, group, world, local, wl, *, steps, warmup, plain_steps, e2e_ste
 
     rec = {"value": value, "unit": "GCUPS", "steps": steps, "warmup": max(warmup, 2),
            "ms_per_step": total_ms / steps, "gpu_launches": launches,
-           "roofline": roofline(cells, sum(score_ms) / steps, dpx, wl, ctx.bits(qdb)),
+           "roofline": roofline(cells, sum(score_ms) / steps, dpx, wl),
            "plain": plain, "batched_over_plain": (value / plain["value"]) if plain else None,
            "e2e": e2e, "overflow_rescored": ovf, "clocks": clocks,
            "config": config_of(wl)}

@@ -747,17 +747,15 @@ def run_ours(args, rank, world, local):
     subs = {}
     if world == 1 and not args.no_sub and args.workload == "16s" and args.nq is None:
         cpu = not args.no_cpu
-        # 10^6 pairs: ~7 ms per step, so enough steps to span several clock samples. Measured
-        # before the protein record: the pairs end-to-end figure is host-bound (packing on the
-        # host threads), and after the protein record's 16-thread CPU baseline it ran slower
-        subs["pairs"] = measure(ctx, group, world, local, workload("pairs"), steps=200, warmup=3,
-                                plain_steps=20, e2e_steps=10, cpu_seconds=5.0 if cpu else 0.0,
-                                dpx=dpx)
         # 4,096 x 100,000 proteins: ~14 s per batched step, ~36 s per plain step
         subs["protein"] = measure(ctx, group, world, local, workload("protein"), steps=2, warmup=3,
                                   plain_steps=1, e2e_steps=1, e2e_warmup=0,
                                   cpu_seconds=6.0 if cpu else 0.0, dpx=dpx,
                                   plain_warm_queries=16)
+        # 10^6 pairs: ~7 ms per step, so enough steps to span several clock samples
+        subs["pairs"] = measure(ctx, group, world, local, workload("pairs"), steps=200, warmup=3,
+                                plain_steps=20, e2e_steps=10, cpu_seconds=5.0 if cpu else 0.0,
+                                dpx=dpx)
         sm = workload("small")
         sm_auto = workload("small")
         sm_auto.scheme = sm.scheme.replace(dtype="auto")

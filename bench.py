@@ -61,6 +61,11 @@ METRIC = "GCUPS on 1 B200 (bit-exact) batched/served vs plain; p50/p99 request l
 # running max issue on the ALU pipe; X + go (vadd2) issues on the FMA pipe.
 ALU_OPS_PER_REG = 4.5
 FMA_OPS_PER_REG = 1.0
+# The inter-sequence pairs kernel (kernels.cuh, inter_strip): a byte permute, E and F add-max
+# and H max3 on the ALU pipe (plus half a running max in local mode), H + s and H + go
+# (vadd2) on the FMA pipe.
+INTER_ALU_OPS_PER_REG = 4.0
+INTER_FMA_OPS_PER_REG = 2.0
 L2_FLUSH_BYTES = 256 << 20
 SERVE_LOADS = "0.5,1,2,4,10,100,2000"
 
@@ -396,10 +401,15 @@ def hbm_peak():
         return 6650.0, "fallback 6.65 TB/s (earlier measurement on this pool)"
 
 
-def roofline(cells, score_ms, dpx, wl=None):
-    """Scoring kernels against the per-pipe instruction ceilings (GCUPS)."""
-    alu = dpx * 2.0 / ALU_OPS_PER_REG / 1e9
-    fma = dpx * 2.0 / FMA_OPS_PER_REG / 1e9
+def roofline(cells, score_ms, dpx, wl=None, inter=False):
+    """Scoring kernels against the per-pipe instruction ceilings (GCUPS). `inter`: the call's
+    pairs ran on the inter-sequence kernel, whose cell costs 4 ALU-pipe ops per register
+    outside local mode."""
+    local = wl is not None and wl.scheme.mode == "local"
+    alu_ops = (INTER_ALU_OPS_PER_REG + (0.5 if local else 0.0)) if inter else ALU_OPS_PER_REG
+    fma_ops = INTER_FMA_OPS_PER_REG if inter else FMA_OPS_PER_REG
+    alu = dpx * 2.0 / alu_ops / 1e9
+    fma = dpx * 2.0 / fma_ops / 1e9
     achieved = cells / (score_ms * 1e-3) / 1e9 if score_ms > 0 else 0.0
     traffic, src = None, ("not extrapolated: no DRAM capture of this kernel at this workload's "
                           "lengths and alphabet")
@@ -408,7 +418,15 @@ def roofline(cells, score_ms, dpx, wl=None):
                "34.3 MB read + 2.6 MB written per launch (0.16 GB/s): the reference streams "
                "are read from DRAM once and then stay in L2, so reads do not grow with the "
                "query count")
-    if wl is not None and wl.name == "pairs" and wl.pairs is not None:
+    if wl is not None and wl.name == "pairs" and wl.pairs is not None and inter:
+        # measured: dram__bytes_read.sum + dram__bytes_write.sum of pairs_inter_kernel on
+        # 300,000 of these pairs = 530,737,664 + 747,239,936 B: 4,259 B per pair, almost all of
+        # it the strip-boundary column (HGO, E per row) written and read back between the five
+        # 32-column strips of a 150-residue read; traffic grows with the pair count
+        traffic = 4259.93 * wl.pairs[0].shape[0]
+        src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of pairs_inter_kernel on "
+               "300,000 pairs of this workload (1,277,977,600 B), scaled by the pair count")
+    if wl is not None and wl.name == "pairs" and wl.pairs is not None and not inter:
         # measured: dram__bytes_read.sum + dram__bytes_write.sum of the pairs kernel on 100,000
         # of these 150/200-residue pairs = 14,885,120 + 0 B (the scores stay in L2 until the
         # launch ends): 148.85 B per pair, the packed words of both sides read once plus the
@@ -418,9 +436,10 @@ def roofline(cells, score_ms, dpx, wl=None):
                "100,000 pairs of this workload (14,885,120 B), scaled by the pair count")
     return {"bound": "int", "achieved": achieved, "peak": alu, "unit": "GCUPS",
             "frac": achieved / alu if alu else None, "peak_pipe": "alu",
+            "kernel": "pairs_inter_kernel" if inter else "team kernels",
             "ceilings_gcups": {"alu": alu, "fma": fma},
             "peak_source": (f"measured s16x2 DPX rate {dpx / 1e12:.2f} T lane-ops/s (live, this GPU)"
-                            f" x 2 cells / {ALU_OPS_PER_REG} ALU-pipe ops per register"),
+                            f" x 2 cells / {alu_ops} ALU-pipe ops per register"),
             "traffic": traffic, "traffic_source": src}
 
 
@@ -452,7 +471,7 @@ def measure(ctx, group, world, local, wl, *, steps, warmup, plain_steps, e2e_ste
     ctx.sync()
     group.barrier()
     sampler = ClockSampler(local).start()
-    times, score_ms, topk_ms, launches, ovf = [], [], [], 0, 0
+    times, score_ms, topk_ms, launches, ovf, inter_items = [], [], [], 0, 0, 0
     for _ in range(steps):
         ctx.flush_l2(L2_FLUSH_BYTES)
         st = step()
@@ -461,6 +480,7 @@ def measure(ctx, group, world, local, wl, *, steps, warmup, plain_steps, e2e_ste
         topk_ms.append(st.last_topk_ms)
         launches += st.last_launches
         ovf += st.last_overflow
+        inter_items = st.last_inter_items
     ctx.sync()
     group.barrier()
     clocks = sampler.stop()
@@ -485,7 +505,7 @@ def measure(ctx, group, world, local, wl, *, steps, warmup, plain_steps, e2e_ste
         plain = {"value": world * cells * plain_steps / (p_ms * 1e-3) / 1e9, "unit": "GCUPS",
                  "steps": plain_steps,
                  "form": ("16 queries per batch with results copied back per batch"
-                          if wl.pairs is None else "pairs in input order") +
+                          if wl.pairs is None else "pairs in input order on the team kernels") +
                          ", one kernel shape per call sized to its longest query, no length"
                          " binning, no CUDA graph; device time"}
 
@@ -534,7 +554,7 @@ def measure(ctx, group, world, local, wl, *, steps, warmup, plain_steps, e2e_ste
 
     rec = {"value": value, "unit": "GCUPS", "steps": steps, "warmup": max(warmup, 2),
            "ms_per_step": total_ms / steps, "gpu_launches": launches,
-           "roofline": roofline(cells, sum(score_ms) / steps, dpx, wl),
+           "roofline": roofline(cells, sum(score_ms) / steps, dpx, wl, inter=inter_items > 0),
            "plain": plain, "batched_over_plain": (value / plain["value"]) if plain else None,
            "e2e": e2e, "overflow_rescored": ovf, "clocks": clocks,
            "config": config_of(wl)}

@@ -700,18 +700,18 @@ template <bool L, bool T>
 void launch_inter_t(gpusw_ctx* c, Bufs& B, gsw::InterParams prm, int max_n, int max_m, const LaunchCfg& lc) {
   auto k = gsw::pairs_inter_kernel<L, T>;
   int bps = 1;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, 256, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, gsw::kInterBlock, 0));
   long long grid = (long long)c->sms * std::max(1, bps);
-  grid = std::max(1ll, std::min(grid, (prm.n_items + 255) / 256));
+  grid = std::max(1ll, std::min(grid, (prm.n_items + gsw::kInterBlock - 1) / gsw::kInterBlock));
   const bool strips = max_n > gsw::kInterW;
-  const size_t need = strips ? (size_t)grid * 256 * (size_t)std::max(1, max_m) : 0;
+  const size_t need = strips ? (size_t)grid * gsw::kInterBlock * (size_t)std::max(1, max_m) : 0;
   if (lc.need) {
     *lc.need = need;
     return;
   }
-  prm.stride = grid * 256;
+  prm.stride = grid * gsw::kInterBlock;
   prm.bnd = strips ? (lc.bnd_off >= 0 ? static_cast<uint2*>(B.bnd.p) + lc.bnd_off : B.bnd.as<uint2>(need)) : nullptr;
-  k<<<(int)grid, 256, 0, lc.st ? lc.st : c->stream>>>(prm);
+  k<<<(int)grid, gsw::kInterBlock, 0, lc.st ? lc.st : c->stream>>>(prm);
   CK(cudaGetLastError());
   c->st.last_launches++;
 }
@@ -795,16 +795,19 @@ InterPlan plan_inter(const Db& q, const Db& r, const int32_t* qi, const int32_t*
   return pl;
 }
 
-// Query length up to which an alignment goes to the inter-sequence kernel (four strips). On
-// uniform read/window-like pairs it measured 2.6x the team kernels at 30 x 40 residues, 1.2x at
-// 60 x 80 and 100 x 120, and 0.9x at 150 x 200, where the team kernel's 160-column pass fits.
-constexpr int kInterMaxCols = 128;
+// Query lengths that go to the inter-sequence kernel. Against the team kernels on uniform
+// pairs (kernel time, semiglobal / local): 30 x 40 2.9x / 2.8x, 100 x 120 1.35x (local),
+// 150 x 200 (10^6 read/window pairs) 1.05x, 160-176 x 220 0.94x / 1.03x, 177-192 x 240
+// 0.88x / 0.94x (the team kernel's 192-column pass is nearly full there), 200-224 x 270
+// 1.10x / 1.05x, 250-256 x 300 0.95x / 0.89x, 384 and 512 columns 0.73-0.76x.
+constexpr int kInterMaxCols = 224;
+bool inter_len(int n) { return n <= 160 || (n > 192 && n <= kInterMaxCols); }
 
 // One thread scores a whole item, so the call takes as long as its longest item unless every
 // resident thread has several: the kernel is used when the items' work is at least twice the
-// largest item's on every resident thread (two 256-thread blocks per SM).
+// largest item's on every resident thread (two blocks per SM).
 bool inter_pays(const gpusw_ctx* c, const InterPlan& pl) {
-  return !pl.items.empty() && pl.work >= 2.0 * (double)c->sms * 512.0 * pl.max_work;
+  return !pl.items.empty() && pl.work >= 2.0 * (double)c->sms * (2.0 * gsw::kInterBlock) * pl.max_work;
 }
 
 // Smallest pairs shape whose columns cover `ncols` and whose profile fits, else the widest
@@ -2365,14 +2368,14 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
     CK(cudaEventRecord(c->ev1, c->stream));
     // Plans the call on the host and runs it (recorded as a graph when cacheable).
     auto plan_and_run = [&](int Pw, bool cacheable) -> Bufs* {
-        // Short alignments (query <= kInterMaxCols) through the inter-sequence kernel when it
+        // Short alignments (query lengths of inter_len) through the inter-sequence kernel when it
         // applies and pays; they take the excluded shape kNumPair below.
         InterPlan ipl;
         bool use_inter = false;
         if (inter_applies(c, q, r, Pw)) {
           std::vector<int> cand;
           for (int64_t i = 0; i < n; ++i)
-            if (q.len[qi[i]] <= kInterMaxCols) cand.push_back((int)i);
+            if (inter_len(q.len[qi[i]])) cand.push_back((int)i);
           if (!cand.empty()) {
             ipl = plan_inter(q, r, qi, rj, cand, local);
             use_inter = inter_pays(c, ipl);
@@ -2407,7 +2410,7 @@ int gpusw_score_pairs(gpusw_ctx* c, int32_t qdb, int32_t rdb, const int32_t* qi,
           for (long long i = lo; i < hi; ++i) {
             const int ql = q.len[qi[i]], rl = r.len[rj[i]];
             const int sh = c->plain ? plain_shape
-                                    : (use_inter && ql <= kInterMaxCols) ? kNumPair
+                                    : (use_inter && inter_len(ql)) ? kNumPair
                                     : (ql <= 4096 ? shape_of_len[ql] : big);
             shp[i] = (uint8_t)sh;
             pt.mrow[sh] = std::max(pt.mrow[sh], rl);

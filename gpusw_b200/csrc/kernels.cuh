@@ -896,6 +896,7 @@ struct InterParams {
 
 constexpr int kInterW = 32;       // columns per strip
 constexpr int kInterTabMax = 65;  // row table words (ns + 1 <= 65)
+constexpr int kInterBlock = 192;  // threads per block: two blocks per SM at up to 170 registers
 
 struct InterItem {
   int n, na, nb, ma, mb, M;
@@ -978,19 +979,9 @@ __device__ __forceinline__ void inter_strip(const InterParams& p, const uint32_t
   uint2 nb = make_uint2(0u, 0u);
   if (!FIRST) nb = *bp;
   const uint32_t v_neg = V<2>::splat(S.neg_low);
-  for (int i = 0; i < it.M; ++i) {
-    const uint32_t ta = TA, tb = TB;
-    if (i + 1 < it.M) row_tab(i + 1, TA, TB);
-    uint32_t hl, e;
-    if (FIRST) {
-      hl = lad;
-      e = NEGF;
-      if (ladder) lad = __vadd2(lad, GE);
-    } else {
-      hl = nb.x;
-      e = nb.y;
-      if (i + 1 < it.M) nb = bp[p.stride];
-    }
+  const uint32_t GEL = ladder ? GE : 0u;
+  // the cells of row i from the row's table words (ta, tb) and left boundary (hl, e)
+  auto cells = [&](uint32_t ta, uint32_t tb, uint32_t hl, uint32_t& e) {
     uint32_t d = dleft, hgo_l = hl;
     dleft = hl;
 #pragma unroll
@@ -1007,13 +998,65 @@ __device__ __forceinline__ void inter_strip(const InterParams& p, const uint32_t
       hgo_l = Hgo[k];
       if (TRACK && (k & 1)) it.acc.best = __vimax3_s16x2(it.acc.best, Hgo[k - 1], Hgo[k]);
     }
+  };
+  auto last_col = [&]() {  // HGO at the query's last column (the last strip only)
+    return dd == 0 ? Hgo[WL4 - 1] : dd == 1 ? Hgo[WL4 - 2] : dd == 2 ? Hgo[WL4 - 3] : Hgo[WL4 - 4];
+  };
+  // Rows before the first capture row, where both halves are live: no branch between rows
+  // (the next row words and boundary entry are loaded unconditionally -- the word after a
+  // sequence lies in the set's slack or its neighbour, the boundary column holds max m rows),
+  // so two rows unrolled give the scheduler two chains of dependent cell updates.
+  const int mfast = max(0, min(it.ma, it.mb) - 1);
+  int i = 0;
+#pragma unroll 2
+  for (; i < mfast; ++i) {
+    const uint32_t ta = TA, tb = TB;
+    TA = s_tab[wa & rmask];  // row i + 1 < min(ma, mb): both halves real
+    TB = s_tab[wb & rmask];
+    wa >>= rbits;
+    wb >>= rbits;
+    const bool rl = ++rpos == rper;
+    rpos = rl ? 0 : rpos;
+    rwa += rl;
+    rwb += rl;
+    const uint32_t la = __ldg(rw + rwa), lb = __ldg(rw + rwb);
+    wa = rl ? la : wa;
+    wb = rl ? lb : wb;
+    uint32_t hl, e;
+    if (FIRST) {
+      hl = lad;
+      e = NEGF;
+      lad = __vadd2(lad, GEL);
+    } else {
+      hl = nb.x;
+      e = nb.y;
+      nb = bp[p.stride];
+    }
+    cells(ta, tb, hl, e);
+    if (!LAST) *bp = make_uint2(Hgo[WL4 - 1], e);
+    bp += p.stride;
+    if (!LOCAL && LAST) it.acc.endcol = __vmaxs2(it.acc.endcol, last_col());
+  }
+  for (; i < it.M; ++i) {
+    const uint32_t ta = TA, tb = TB;
+    if (i + 1 < it.M) row_tab(i + 1, TA, TB);
+    uint32_t hl, e;
+    if (FIRST) {
+      hl = lad;
+      e = NEGF;
+      lad = __vadd2(lad, GEL);
+    } else {
+      hl = nb.x;
+      e = nb.y;
+      if (i + 1 < it.M) nb = bp[p.stride];
+    }
+    cells(ta, tb, hl, e);
     if (!LAST) *bp = make_uint2(Hgo[WL4 - 1], e);
     bp += p.stride;
     if (!LOCAL) {
-      if (LAST && S.mode == kModeSemi && S.free_q) {  // H(i, n) of the rows each half has
-        const uint32_t v = dd == 0 ? Hgo[WL4 - 1] : dd == 1 ? Hgo[WL4 - 2] : dd == 2 ? Hgo[WL4 - 3] : Hgo[WL4 - 4];
+      if (LAST) {  // H(i, n) of the rows each half has (used for a free query end)
         const uint32_t live = (i < it.ma ? 0x0000FFFFu : 0u) | (i < it.mb ? 0xFFFF0000u : 0u);
-        it.acc.endcol = __vmaxs2(it.acc.endcol, (v & live) | (v_neg & ~live));
+        it.acc.endcol = __vmaxs2(it.acc.endcol, (last_col() & live) | (v_neg & ~live));
       }
       if (i == it.ma - 1 || i == it.mb - 1) {  // a half's last row: corner and last-row maximum
         const uint32_t half = (i == it.ma - 1 ? 0x0000FFFFu : 0u) | (i == it.mb - 1 ? 0xFFFF0000u : 0u);
@@ -1022,10 +1065,7 @@ __device__ __forceinline__ void inter_strip(const InterParams& p, const uint32_t
         for (int k = 0; k < WL4; ++k)
           if (!LAST || k < WL4 - 4 || k < WL4 - dd) rmax = __vmaxs2(rmax, Hgo[k]);
         it.acc.endrow = __vmaxs2(it.acc.endrow, (rmax & half) | (v_neg & ~half));
-        if (LAST) {
-          const uint32_t v = dd == 0 ? Hgo[WL4 - 1] : dd == 1 ? Hgo[WL4 - 2] : dd == 2 ? Hgo[WL4 - 3] : Hgo[WL4 - 4];
-          it.acc.corner = (v & half) | (it.acc.corner & ~half);
-        }
+        if (LAST) it.acc.corner = (last_col() & half) | (it.acc.corner & ~half);
       }
     }
   }
@@ -1050,11 +1090,15 @@ __device__ __forceinline__ void inter_last_strip(const InterParams& p, const uin
 // Persistent: each warp takes 32 consecutive items per queue step (one per lane); the host
 // orders items by query length then reference length, longest first, so a warp's lanes run
 // strips of the same widths over similar row counts.
+//
+// 192-thread blocks: the strip's HGO and F (64 registers), two rows in flight and the row
+// state take 160-170 registers, spill-free only under a cap above 128; at 256 threads (cap
+// 128) the kernel spilled and ran 0-13 % slower.
 template <bool LOCAL, bool TRACK>
-__global__ void __launch_bounds__(256, 2) pairs_inter_kernel(const InterParams p) {
+__global__ void __launch_bounds__(kInterBlock, 2) pairs_inter_kernel(const InterParams p) {
   static_assert(kInterW == 32, "two packed query words per strip");
   __shared__ uint32_t s_tab[kInterTabMax];
-  __shared__ uint4 s_qsel[kInterW / 4 * 256];
+  __shared__ uint4 s_qsel[kInterW / 4 * kInterBlock];
   uint4* s_q = s_qsel + threadIdx.x;
   const SchemeDev& S = p.S;
   for (int r = threadIdx.x; r <= S.ns; r += blockDim.x) {

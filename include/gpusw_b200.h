@@ -186,9 +186,9 @@ int gpusw_locate_pairs(gpusw_ctx *ctx, int32_t qdb, int32_t rdb, const int32_t *
  * launch per shape on up to four streams (the default: on the uneven-length protein top-10
  * the single launch measured 7 % slower, its registers being the most any shape needs),
  * GPUSW_OPT_NO_INTER keeps every explicit pair on the team kernels (by default, int16 pairs
- * of queries up to 128 residues go to the inter-sequence kernel, one thread per two
- * alignments, when the query set holds only codes 0..3, the scheme's values fit a byte and
- * the call has enough of them to keep every thread busy). */
+ * of queries up to 160 residues or of 193 to 224 go to the inter-sequence kernel, one thread
+ * per two alignments, when the query set holds only codes 0..3, the scheme's values fit a
+ * byte and the call has enough of them to keep every thread busy). */
 #define GPUSW_OPT_NO_AUTOTUNE 1
 #define GPUSW_OPT_NO_GRAPHS 2
 #define GPUSW_OPT_ONE_LAUNCH 4

@@ -1,8 +1,8 @@
 """The inter-sequence pairs kernel (pairs_inter_kernel: one thread scores two alignments as the
-int16 halves of its registers): explicit int16 pairs of queries up to 128 residues go to it
+int16 halves of its registers): explicit int16 pairs of queries up to 160 residues or of 193 to 224 go to it
 when the call has enough of them. Every case is checked against the team kernels (the same
 call with the kernel switched off) on all pairs and against the C oracle on a sample, across
-modes and free-end flags, strip boundaries (1..128 columns), uneven references, empty
+modes and free-end flags, strip boundaries (1..224 columns), uneven references, empty
 sequences, sentinel codes in references, and calls that mix both kernels."""
 import numpy as np
 import pytest
@@ -68,9 +68,10 @@ def test_inter_uniform_short_pairs(sch):
     assert items >= n // 2
 
 
-@pytest.mark.parametrize("lo,hi", [(1, 8), (29, 36), (95, 128)], ids=["1-8", "29-36", "95-128"])
+@pytest.mark.parametrize("lo,hi", [(1, 8), (29, 36), (95, 128), (190, 224)],
+                         ids=["1-8", "29-36", "95-128", "190-224"])
 def test_inter_strip_widths_and_ends(lo, hi):
-    """Every last-strip width (1..32 columns, 1..4 strips); references of 100..150 rows and
+    """Every last-strip width (1..32 columns, 1..7 strips); references of 100..150 rows and
     0.5 % empty queries and references."""
     rng = np.random.default_rng(71 + lo)
     n = 900_077
@@ -100,7 +101,7 @@ def test_inter_mixed_call_and_routing():
     n = 1_000_000
     q, r = _set(rng, n, 20, 120), _set(rng, n, 60, 120)
     ql = np.diff(q[1]).copy()
-    long_q = _set(rng, 20_000, 129, 400)
+    long_q = _set(rng, 20_000, 225, 400)
     codes = np.concatenate([q[0], long_q[0]])
     offs = np.concatenate([q[1], long_q[1][1:] + q[1][-1]]).astype(np.int32)
     qi = np.arange(n + 20_000, dtype=np.int32)

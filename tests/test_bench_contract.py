@@ -43,6 +43,30 @@ def test_roofline_binds_on_the_alu_pipe():
     assert r["traffic"] is None  # cross products: L2-resident references, not extrapolated
 
 
+def test_roofline_of_the_inter_sequence_pairs_kernel():
+    """Pairs scored by the inter-sequence kernel are measured against its own ceiling: 4 ALU
+    ops per register outside local mode (4.5 with the running maximum), 2 vadd2 on the FMA
+    pipe; the pairs workload's traffic is the measured DRAM bytes of that kernel per pair."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    rate = 18.48e12
+    wl = bench.workload("pairs", nq=1000)
+    assert wl.scheme.mode == "semiglobal"
+    r = bench.roofline(cells=wl.cells(), score_ms=1.0, dpx=rate, wl=wl, inter=True)
+    assert r["kernel"] == "pairs_inter_kernel"
+    assert abs(r["peak"] - rate * 2 / 4.0 / 1e9) < 1e-6
+    assert abs(r["ceilings_gcups"]["fma"] - rate * 2 / 2.0 / 1e9) < 1e-6
+    assert abs(r["traffic"] - 4259.93 * 1000) < 1e-3 and "pairs_inter_kernel" in r["traffic_source"]
+    team = bench.roofline(cells=wl.cells(), score_ms=1.0, dpx=rate, wl=wl, inter=False)
+    assert team["kernel"] == "team kernels" and abs(team["peak"] - rate * 2 / 4.5 / 1e9) < 1e-6
+    assert abs(team["traffic"] - 148.8512 * 1000) < 1e-3
+    local = wl.scheme.replace(mode="local")
+    wl.scheme = local
+    r_local = bench.roofline(cells=1.0, score_ms=1.0, dpx=rate, wl=wl, inter=True)
+    assert abs(r_local["peak"] - rate * 2 / 4.5 / 1e9) < 1e-6
+
+
 def test_reference_code_baseline_matches_the_oracle():
     """The reference package's own cpu_reference_score (installed under baseline/_ref), run
     in a spawn pool, gives the C oracle's scores on a seeded sample of the small workload."""
